@@ -1,0 +1,198 @@
+/*
+ * knng.h -- C ABI of the B200 k-NN graph builder (libknng.so).
+ *
+ * The library builds an approximate k-nearest-neighbour graph (squared L2) with
+ * the method of the reference's SolutionKmeans: repeated recursive 2-means
+ * splitting of the point set into buckets, an all-pairs pass inside every
+ * bucket into a bounded per-point neighbour set, and an optional
+ * neighbour-of-neighbour refinement pass.  Every stage runs as sm_100a CUDA
+ * kernels; the host code only sequences them.
+ *
+ * The reference has no plugin or FFI layer: its boundary is C++ linkage to
+ * header-only static members called by main() (src/main.cpp:59).  Each entry
+ * point below names the reference function it replaces.
+ *
+ * Conventions
+ *   - Every call returns a knng_status; nothing throws across the ABI.
+ *   - Points are row-major float32, n rows of d values, row stride ld_bytes
+ *     (ld_bytes >= 4*d).  Host pointers unless the name says _device.
+ *   - Output rows are sorted by (distance, id) ascending; rows with fewer than
+ *     k neighbours are padded with id 1 (distance +inf), as padResult does.
+ *   - A context is not re-entrant: one host thread at a time.  Use several
+ *     contexts for concurrency.
+ *   - Arithmetic: squared distances and hyperplane side tests use the
+ *     reference's FP32 evaluation order (8 FMA lanes over dims l, l+8, ...,
+ *     lanes summed left to right, tail dims added one by one), so given the
+ *     same hyperplanes and buckets the results are bit-identical to the
+ *     reference's.
+ */
+#ifndef KNNG_H
+#define KNNG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct knng_context knng_context;
+
+typedef enum knng_status {
+    KNNG_OK = 0,
+    KNNG_ERR_INVALID_ARGUMENT = 1, /* null pointer, size out of range, bad stride */
+    KNNG_ERR_CUDA = 2,             /* a CUDA runtime call failed; see knng_last_error */
+    KNNG_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed */
+    KNNG_ERR_BUDGET = 4,           /* the request exceeds the context's HBM budget */
+    KNNG_ERR_STATE = 5,            /* call out of order, e.g. no points loaded */
+    KNNG_ERR_UNSUPPORTED = 6,      /* d or k outside the compiled set */
+    KNNG_ERR_NO_DEVICE = 7         /* no CUDA device, or the device is not sm_100 */
+} knng_status;
+
+enum {
+    KNNG_PRECISION_FP32 = 0,       /* exact FP32 distances everywhere (bit-exact form) */
+    KNNG_PRECISION_BF16_RERANK = 1 /* reserved: BF16 tensor-core distances + FP32 re-rank */
+};
+
+/* Build parameters.  knng_default_params() fills the reference's values. */
+typedef struct knng_params {
+    uint32_t k;               /* neighbours per point, 1..128 (reference k = 100, src/Constants.hpp:24) */
+    uint32_t max_leaf;        /* a node is a bucket iff its size < max_leaf (maxGroupSize,
+                                 src/SolutionKmeans.hpp:152); reference alternates 200/400 */
+    uint32_t max_leaf_odd;    /* if nonzero, odd repetitions use this max_leaf (the 200/400
+                                 alternation of src/SolutionKmeans.hpp:582-587); 0 = max_leaf */
+    uint32_t lloyd_iters;     /* 2-means iterations per split (knnIterations, :591) */
+    uint32_t reps;            /* repetitions of split + bucket pass (the loop at :579-602) */
+    uint32_t refine;          /* 1 = run the neighbour-of-neighbour pass (topUpSingle, :604) */
+    uint32_t small_threshold; /* nodes below this size run Lloyd over all their points (:156, 3000) */
+    uint32_t precision;       /* KNNG_PRECISION_* */
+    uint64_t seed;            /* keys the device's counter-based RNG */
+} knng_params;
+
+/* Per-call statistics.  Times come from CUDA events on the context's stream. */
+typedef struct knng_stats {
+    double ms_total;          /* whole call, device time */
+    double ms_split;          /* tree construction (seeding, Lloyd, side test, partition) */
+    double ms_leaf;           /* bucket all-pairs + neighbour-set updates */
+    double ms_leaf_kernel;    /* sum of bucket-kernel durations alone */
+    double ms_refine;         /* neighbour-of-neighbour pass */
+    double ms_finalize;       /* sort + pad */
+    uint64_t reps_done;
+    uint64_t split_levels;    /* tree levels over all repetitions */
+    uint64_t split_nodes;     /* nodes split over all repetitions */
+    uint64_t restarts;        /* split attempts repeated (empty cluster / side) */
+    uint64_t fallback_splits; /* nodes split at the index midpoint after repeated failure */
+    uint64_t buckets;         /* buckets processed over all repetitions */
+    uint64_t bucket_pairs;    /* sum over buckets of b*(b-1)/2 */
+    uint64_t bucket_pair_evals; /* distances the bucket kernel evaluated (ordered pairs) */
+    uint64_t leaf_launches;   /* bucket-kernel launches */
+    uint64_t kernel_launches; /* all kernels launched by the call */
+    uint64_t refine_changed;  /* points whose set changed in the refinement pass */
+} knng_stats;
+
+/* Fills the reference's parameters: k=100, max_leaf=200, max_leaf_odd=400,
+ * lloyd_iters=1, reps=8, refine=1, small_threshold=3000, FP32, seed=12345. */
+void knng_default_params(knng_params* params);
+
+const char* knng_status_string(knng_status status);
+
+/* Creates a context on CUDA device `device`.  hbm_budget_bytes caps the
+ * device memory the context may hold (0 = 90% of the device's memory). */
+knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** out);
+knng_status knng_destroy(knng_context* ctx);
+
+/* Last error message of this context ("" if none). */
+const char* knng_last_error(const knng_context* ctx);
+
+/* ---------------------------------------------------------------- one call
+ * Replaces SolutionKmeans::constructResult(points, numPoints, result)
+ * (src/SolutionKmeans.hpp:558-616) with fixed repetition count instead of a
+ * wall-clock budget.  out_ids: n*k uint32 (required); out_dists: n*k float
+ * (optional, may be NULL); stats optional. */
+knng_status knng_build(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                       const knng_params* params, uint32_t* out_ids, float* out_dists, knng_stats* stats);
+
+/* The same with device-resident input and output (pointers into the
+ * context's device memory space); synchronous. */
+knng_status knng_build_device(knng_context* ctx, const float* d_points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                              const knng_params* params, uint32_t* d_out_ids, float* d_out_dists,
+                              knng_stats* stats);
+
+/* ---------------------------------------------------------------- stepwise
+ * The stages one at a time, so that each can be fed the reference's
+ * intermediate state and compared with it. */
+
+/* Loads n points (copied into the context; on_device != 0: `points` is a
+ * device pointer).  Resets indices to 0..n-1 and clears the neighbour sets. */
+knng_status knng_load_points(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                             int on_device);
+
+/* Clears every neighbour set and sets its capacity to k (1..128). */
+knng_status knng_reset_sets(knng_context* ctx, uint32_t k);
+
+/* indices = 0..n-1 (the std::iota at src/SolutionKmeans.hpp:589). */
+knng_status knng_begin_rep(knng_context* ctx);
+
+/* Stable partition of indices[starts[i], ends[i]) for `count` disjoint nodes,
+ * by side = dot(coefs[i], point) >= offsets[i] with side-true points first
+ * (the final-groups step, src/SolutionKmeans.hpp:188-205 and :262-304).
+ * coefs: count*d floats.  out_mids[i] = starts[i] + number of side-true points. */
+knng_status knng_split_nodes(knng_context* ctx, uint32_t count, const uint32_t* starts, const uint32_t* ends,
+                             const float* coefs, const float* offsets, uint32_t* out_mids);
+
+/* Farthest pair among the points at positions[offsets[i] .. offsets[i+1])
+ * of indices (kmeansStartVecs, src/SolutionKmeans.hpp:68-138): out_first /
+ * out_second are offsets into that list; out_ok[i] = 0 when no pair has a
+ * distance above FLT_MIN. */
+knng_status knng_farthest_pair(knng_context* ctx, uint32_t count, const uint64_t* offsets,
+                               const uint32_t* positions, uint32_t* out_first, uint32_t* out_second,
+                               int32_t* out_ok);
+
+/* `iters` 2-means iterations per node from the given starting centres, over
+ * the positions in lloyd_offsets/lloyd_positions, or over the whole node
+ * [starts[i], ends[i]) when that node's list is empty (the Lloyd loops at
+ * src/SolutionKmeans.hpp:161-186 and :218-260), then the final hyperplane.
+ * out_ok[i] = 0 when an iteration left a cluster empty. */
+knng_status knng_lloyd(knng_context* ctx, uint32_t count, const uint32_t* starts, const uint32_t* ends,
+                       const uint64_t* lloyd_offsets, const uint32_t* lloyd_positions, const float* c1_start,
+                       const float* c2_start, uint32_t iters, float* out_coefs, float* out_offsets,
+                       int32_t* out_ok);
+
+/* All-pairs pass over buckets [starts[i], ends[i]) of the current indices
+ * (addCandidatesLessThan, src/KnnSets.hpp:131-160). */
+knng_status knng_process_leaves(knng_context* ctx, uint32_t count, const uint32_t* starts, const uint32_t* ends);
+
+/* One full device-seeded repetition: indices = iota, level-synchronous
+ * recursive split, then every bucket (splitKmeansBinaryProcess,
+ * src/SolutionKmeans.hpp:142-311).  rep_index keys the RNG. */
+knng_status knng_run_rep(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold,
+                         uint64_t seed, uint32_t rep_index, knng_stats* stats);
+
+/* Leaf ranges of the last knng_run_rep, in position order. */
+knng_status knng_get_leaves(knng_context* ctx, uint32_t capacity, uint32_t* starts, uint32_t* ends,
+                            uint32_t* out_count);
+
+/* Neighbour-of-neighbour pass (topUpSingle, src/SolutionKmeans.hpp:480-555),
+ * candidates offered in ascending id order.  out_changed may be NULL. */
+knng_status knng_refine(knng_context* ctx, uint64_t* out_changed);
+
+knng_status knng_get_indices(knng_context* ctx, uint32_t* out);
+knng_status knng_set_indices(knng_context* ctx, const uint32_t* in);
+
+/* Raw neighbour-set state in slot order (the fields of KnnSetScannableSimd,
+ * src/KnnSets.hpp:26-31): dist/ids n*k, size n, maxslot n (0xFFFFFFFF while
+ * not full), bound n (FLT_MAX while not full).  Any pointer may be NULL. */
+knng_status knng_get_sets(knng_context* ctx, float* dist, uint32_t* ids, uint32_t* sizes, uint32_t* maxslot,
+                          float* bounds);
+knng_status knng_set_sets(knng_context* ctx, const float* dist, const uint32_t* ids, const uint32_t* sizes,
+                          const uint32_t* maxslot, const float* bounds);
+
+/* Sorted, padded output (finalize + padResult, src/KnnSets.hpp:113-126,
+ * :334-344): out_ids n*k, out_dists n*k (may be NULL). Host pointers. */
+knng_status knng_finalize(knng_context* ctx, uint32_t* out_ids, float* out_dists);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KNNG_H */

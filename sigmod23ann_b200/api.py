@@ -1,0 +1,304 @@
+"""Python host mirror of the C ABI in include/knng.h (ctypes over libknng.so).
+
+The reference's entry point is ``SolutionKmeans::constructResult(points,
+numPoints, result)`` (src/SolutionKmeans.hpp:558); :func:`construct_result`
+mirrors it.  :class:`KnngContext` exposes every stage separately so tests can
+feed the reference's intermediate state (hyperplanes, buckets, sets) and
+compare.  There is no CPU fallback: if libknng.so is missing or no sm_100
+device is present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int, c_int32, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libknng.so")
+
+KNNG_OK = 0
+STATUS_NAMES = {
+    0: "KNNG_OK", 1: "KNNG_ERR_INVALID_ARGUMENT", 2: "KNNG_ERR_CUDA", 3: "KNNG_ERR_OUT_OF_MEMORY",
+    4: "KNNG_ERR_BUDGET", 5: "KNNG_ERR_STATE", 6: "KNNG_ERR_UNSUPPORTED", 7: "KNNG_ERR_NO_DEVICE",
+}
+PRECISION_FP32 = 0
+PRECISION_BF16_RERANK = 1
+
+# Every symbol include/knng.h declares (checked by the CPU test suite).
+EXPORTED = [
+    "knng_default_params", "knng_status_string", "knng_create", "knng_destroy", "knng_last_error", "knng_build",
+    "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
+    "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
+    "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
+]
+
+
+class Params(Structure):
+    _fields_ = [
+        ("k", c_uint32), ("max_leaf", c_uint32), ("max_leaf_odd", c_uint32), ("lloyd_iters", c_uint32),
+        ("reps", c_uint32), ("refine", c_uint32), ("small_threshold", c_uint32), ("precision", c_uint32),
+        ("seed", c_uint64),
+    ]
+
+
+class Stats(Structure):
+    _fields_ = [
+        ("ms_total", c_double), ("ms_split", c_double), ("ms_leaf", c_double), ("ms_leaf_kernel", c_double),
+        ("ms_refine", c_double), ("ms_finalize", c_double),
+        ("reps_done", c_uint64), ("split_levels", c_uint64), ("split_nodes", c_uint64), ("restarts", c_uint64),
+        ("fallback_splits", c_uint64), ("buckets", c_uint64), ("bucket_pairs", c_uint64),
+        ("bucket_pair_evals", c_uint64), ("leaf_launches", c_uint64), ("kernel_launches", c_uint64),
+        ("refine_changed", c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class KnngError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libknng.so (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: run `python -m sigmod23ann_b200.build`")
+    lib = ctypes.CDLL(path)
+    P = c_void_p
+    sigs = {
+        "knng_default_params": (None, [POINTER(Params)]),
+        "knng_status_string": (c_char_p, [c_int]),
+        "knng_create": (c_int, [c_int, c_uint64, POINTER(c_void_p)]),
+        "knng_destroy": (c_int, [P]),
+        "knng_last_error": (c_char_p, [P]),
+        "knng_build": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), P, P, POINTER(Stats)]),
+        "knng_build_device": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), P, P, POINTER(Stats)]),
+        "knng_load_points": (c_int, [P, P, c_uint32, c_uint32, c_uint64, c_int]),
+        "knng_reset_sets": (c_int, [P, c_uint32]),
+        "knng_begin_rep": (c_int, [P]),
+        "knng_split_nodes": (c_int, [P, c_uint32, P, P, P, P, P]),
+        "knng_farthest_pair": (c_int, [P, c_uint32, P, P, P, P, P]),
+        "knng_lloyd": (c_int, [P, c_uint32, P, P, P, P, P, P, c_uint32, P, P, P]),
+        "knng_process_leaves": (c_int, [P, c_uint32, P, P]),
+        "knng_run_rep": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, c_uint32, POINTER(Stats)]),
+        "knng_get_leaves": (c_int, [P, c_uint32, P, P, P]),
+        "knng_refine": (c_int, [P, P]),
+        "knng_get_indices": (c_int, [P, P]),
+        "knng_set_indices": (c_int, [P, P]),
+        "knng_get_sets": (c_int, [P, P, P, P, P, P]),
+        "knng_set_sets": (c_int, [P, P, P, P, P, P]),
+        "knng_finalize": (c_int, [P, P, P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def default_params(**overrides) -> Params:
+    p = Params()
+    load_library().knng_default_params(ctypes.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(c_void_p)
+    if isinstance(a, int):
+        return c_void_p(a)
+    return c_void_p(a.data_ptr())  # torch tensor
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class KnngContext:
+    """One device context (not re-entrant)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self._lib = load_library()
+        h = c_void_p()
+        self._check(self._lib.knng_create(device, hbm_budget_bytes, ctypes.byref(h)), ctx=None)
+        self._h = h
+        self.n = 0
+        self.d = 0
+        self.k = 0
+
+    # ------------------------------------------------------------- plumbing
+    def _check(self, status: int, ctx="self"):
+        if status != KNNG_OK:
+            msg = ""
+            if ctx is not None and getattr(self, "_h", None):
+                raw = self._lib.knng_last_error(self._h)
+                msg = raw.decode() if raw else ""
+            if not msg:
+                msg = self._lib.knng_status_string(status).decode()
+            raise KnngError(status, msg)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.knng_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------- one call
+    def build(self, points: np.ndarray, params: Params | None = None, want_dists: bool = False,
+              stats: Stats | None = None):
+        pts = _f32(points)
+        n, d = pts.shape
+        p = params or default_params()
+        ids = np.empty((n, p.k), np.uint32)
+        dists = np.empty((n, p.k), np.float32) if want_dists else None
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_build(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p), _ptr(ids),
+                                         _ptr(dists), ctypes.byref(st)))
+        self.n, self.d, self.k = n, d, p.k
+        return (ids, dists) if want_dists else ids
+
+    def build_device(self, points_ptr: int, n: int, d: int, out_ids_ptr: int, out_dists_ptr: int | None = None,
+                     params: Params | None = None, stats: Stats | None = None, ld_bytes: int = 0) -> Stats:
+        """Device-resident build: pointers are device addresses (e.g. torch data_ptr())."""
+        p = params or default_params()
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_build_device(self._h, c_void_p(points_ptr), n, d, ld_bytes or 4 * d,
+                                                ctypes.byref(p), c_void_p(out_ids_ptr),
+                                                c_void_p(out_dists_ptr) if out_dists_ptr else None,
+                                                ctypes.byref(st)))
+        self.n, self.d, self.k = n, d, p.k
+        return st
+
+    # ------------------------------------------------------------- stepwise
+    def load_points(self, points: np.ndarray) -> None:
+        pts = _f32(points)
+        self.n, self.d = pts.shape
+        self._check(self._lib.knng_load_points(self._h, _ptr(pts), self.n, self.d, pts.strides[0], 0))
+
+    def reset_sets(self, k: int) -> None:
+        self._check(self._lib.knng_reset_sets(self._h, k))
+        self.k = k
+
+    def begin_rep(self) -> None:
+        self._check(self._lib.knng_begin_rep(self._h))
+
+    def split_nodes(self, starts, ends, coefs, offsets) -> np.ndarray:
+        s, e, c, o = _u32(starts), _u32(ends), _f32(coefs), _f32(offsets)
+        mids = np.zeros(len(s), np.uint32)
+        self._check(self._lib.knng_split_nodes(self._h, len(s), _ptr(s), _ptr(e), _ptr(c), _ptr(o), _ptr(mids)))
+        return mids
+
+    def farthest_pair(self, offsets, positions):
+        off = np.ascontiguousarray(offsets, np.uint64)
+        pos = _u32(positions)
+        m = len(off) - 1
+        f = np.zeros(m, np.uint32)
+        s = np.zeros(m, np.uint32)
+        ok = np.zeros(m, np.int32)
+        self._check(self._lib.knng_farthest_pair(self._h, m, _ptr(off), _ptr(pos), _ptr(f), _ptr(s), _ptr(ok)))
+        return f, s, ok
+
+    def lloyd(self, starts, ends, lloyd_offsets, lloyd_positions, c1, c2, iters: int):
+        s, e = _u32(starts), _u32(ends)
+        off = np.ascontiguousarray(lloyd_offsets, np.uint64)
+        pos = _u32(lloyd_positions)
+        a, b = _f32(c1), _f32(c2)
+        m = len(s)
+        coefs = np.zeros((m, self.d), np.float32)
+        offs = np.zeros(m, np.float32)
+        ok = np.zeros(m, np.int32)
+        self._check(self._lib.knng_lloyd(self._h, m, _ptr(s), _ptr(e), _ptr(off), _ptr(pos), _ptr(a), _ptr(b),
+                                         iters, _ptr(coefs), _ptr(offs), _ptr(ok)))
+        return coefs, offs, ok
+
+    def process_leaves(self, starts, ends) -> None:
+        s, e = _u32(starts), _u32(ends)
+        self._check(self._lib.knng_process_leaves(self._h, len(s), _ptr(s), _ptr(e)))
+
+    def run_rep(self, max_leaf: int, lloyd_iters: int, small_threshold: int = 3000, seed: int = 12345,
+                rep_index: int = 0, stats: Stats | None = None) -> Stats:
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_run_rep(self._h, max_leaf, lloyd_iters, small_threshold, seed, rep_index,
+                                           ctypes.byref(st)))
+        return st
+
+    def leaves(self):
+        cnt = c_uint32()
+        self._check(self._lib.knng_get_leaves(self._h, 0, None, None, ctypes.byref(cnt)))
+        s = np.zeros(cnt.value, np.uint32)
+        e = np.zeros(cnt.value, np.uint32)
+        self._check(self._lib.knng_get_leaves(self._h, cnt.value, _ptr(s), _ptr(e), ctypes.byref(cnt)))
+        return s, e
+
+    def refine(self) -> int:
+        out = np.zeros(1, np.uint64)
+        self._check(self._lib.knng_refine(self._h, _ptr(out)))
+        return int(out[0])
+
+    def indices(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint32)
+        self._check(self._lib.knng_get_indices(self._h, _ptr(out)))
+        return out
+
+    def set_indices(self, idx) -> None:
+        a = _u32(idx)
+        self._check(self._lib.knng_set_indices(self._h, _ptr(a)))
+
+    def sets(self) -> dict:
+        n, k = self.n, self.k
+        out = {
+            "dist": np.zeros((n, k), np.float32), "id": np.zeros((n, k), np.uint32),
+            "size": np.zeros(n, np.uint32), "maxslot": np.zeros(n, np.uint32), "bound": np.zeros(n, np.float32),
+        }
+        self._check(self._lib.knng_get_sets(self._h, *(_ptr(out[x]) for x in ("dist", "id", "size", "maxslot",
+                                                                              "bound"))))
+        return out
+
+    def set_sets(self, s: dict) -> None:
+        arrs = [_f32(s["dist"]), _u32(s["id"]), _u32(s["size"]), _u32(s["maxslot"]), _f32(s["bound"])]
+        self._check(self._lib.knng_set_sets(self._h, *(_ptr(a) for a in arrs)))
+
+    def finalize(self, want_dists: bool = False):
+        ids = np.zeros((self.n, self.k), np.uint32)
+        dists = np.zeros((self.n, self.k), np.float32) if want_dists else None
+        self._check(self._lib.knng_finalize(self._h, _ptr(ids), _ptr(dists)))
+        return (ids, dists) if want_dists else ids
+
+
+def construct_result(points: np.ndarray, params: Params | None = None, device: int = 0) -> np.ndarray:
+    """SolutionKmeans::constructResult (src/SolutionKmeans.hpp:558-616) on the GPU:
+    returns the n x k neighbour ids, sorted by (distance, id), short rows padded with id 1."""
+    with KnngContext(device) as ctx:
+        return ctx.build(points, params)

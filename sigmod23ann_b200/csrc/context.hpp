@@ -1,0 +1,126 @@
+// Host-side state of one knng_context: device buffers, the stream, error
+// reporting, and the launchers every .cu file provides.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/knng.h"
+
+namespace knng {
+
+// Thrown inside the library only; every C entry point converts it to a status.
+struct Error {
+    knng_status status;
+    std::string message;
+};
+
+[[noreturn]] void fail(knng_status s, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+#define KNNG_CUDA(call) ::knng::check_cuda((call), #call)
+
+// A typed device allocation owned by the context; counts toward the budget.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct Timer {
+    cudaEvent_t start = nullptr, stop = nullptr;
+};
+
+struct Context {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t held = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+
+    // Points: n rows of ld floats (ld = d rounded up to 4), 16-byte aligned.
+    uint32_t n = 0, d = 0, ld = 0;
+    float* points = nullptr;
+    bool points_borrowed = false;  // true when `points` is the caller's device buffer
+
+    // Permutation of point ids; a second buffer for the partition scatter.
+    uint32_t* indices = nullptr;
+    uint32_t* indices_tmp = nullptr;
+
+    // Neighbour sets, slot order, capacity k per point.
+    uint32_t k = 0;
+    float* set_dist = nullptr;
+    uint32_t* set_id = nullptr;
+    uint32_t* set_size = nullptr;
+    uint32_t* set_maxslot = nullptr;
+    float* set_bound = nullptr;
+
+    // Leaves of the last device-seeded repetition.
+    std::vector<uint32_t> last_leaf_start, last_leaf_end;
+
+    // Named scratch allocations, grown on demand and reused across calls.
+    std::vector<std::pair<std::string, DeviceBuffer>> scratch;
+
+    uint64_t launches = 0;
+};
+
+// Allocation helpers (budget-checked).
+void* dev_alloc(Context& c, size_t bytes);
+void dev_free(Context& c, void* p, size_t bytes);
+void* scratch(Context& c, const char* name, size_t bytes);
+void release_all(Context& c);
+
+// Uploads `count` elements into named scratch and returns the device pointer.
+template <class T>
+T* upload(Context& c, const char* name, const T* host, size_t count) {
+    T* d = static_cast<T*>(scratch(c, name, count * sizeof(T) + 16));
+    if (count) KNNG_CUDA(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    return d;
+}
+
+template <class T>
+void download(Context& c, T* host, const T* dev, size_t count) {
+    if (count) KNNG_CUDA(cudaMemcpyAsync(host, dev, count * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+    KNNG_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+bool dim_supported(uint32_t d);
+
+// ----------------------------------------------------------- launchers
+// split.cu
+void launch_iota(Context& c);
+// Counter-RNG draws for `count` nodes: node i draws (draw_off[i+1]-draw_off[i])
+// positions; the first seed-list-length of them go to d_seeds (CSR seed_off),
+// the first Lloyd-list-length to d_lloyd (CSR lloyd_off).
+void launch_draw_positions(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
+                           const uint32_t* d_attempts, const uint64_t* d_draw_off, const uint64_t* d_seed_off,
+                           const uint64_t* d_lloyd_off, uint64_t seed, uint32_t rep, uint32_t* d_seeds,
+                           uint32_t* d_lloyd);
+// Dense copy of the hyperplanes of the picked nodes.
+void launch_gather_planes(Context& c, const float* d_coefs, const float* d_offsets, const uint32_t* d_pick,
+                          uint32_t count, float* d_out_coefs, float* d_out_offsets);
+// Farthest pair per node over a CSR position list; writes the two rows to
+// d_c1 / d_c2 (count*ld floats) and d_ok = 0 where no pair exceeds FLT_MIN.
+void launch_farthest_pair(Context& c, uint32_t count, const uint64_t* d_offsets, const uint32_t* d_positions,
+                          uint32_t max_list, uint32_t* d_first, uint32_t* d_second, int32_t* d_ok, float* d_c1,
+                          float* d_c2);
+// `iters` Lloyd iterations per node over its CSR list (or its whole range when
+// the list is empty), then the final hyperplane into d_coefs / d_offsets.
+void launch_lloyd(Context& c, uint32_t count, const uint32_t* h_starts, const uint32_t* h_ends,
+                  const uint64_t* h_lloyd_offsets, const uint32_t* d_lloyd_positions, float* d_c1, float* d_c2,
+                  uint32_t iters, float* d_coefs, float* d_offsets, int32_t* d_ok);
+// Side test + stable partition of `count` disjoint nodes; d_true[i] receives
+// the number of side-true points of node i.
+void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, const uint32_t* h_ends,
+                      const uint32_t* d_starts, const float* d_coefs, const float* d_offsets, uint32_t* d_true);
+// leaf.cu
+void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
+                   uint32_t max_bucket, uint64_t* evals);
+// refine.cu
+uint64_t run_refine(Context& c);
+// finalize.cu
+void launch_finalize(Context& c, uint32_t* d_ids, float* d_dists);
+void launch_reset_sets(Context& c);
+
+}  // namespace knng

@@ -1,0 +1,174 @@
+// Bucket all-pairs kernel: addCandidatesLessThan (src/KnnSets.hpp:131-160)
+// for every bucket of a repetition at once, one CTA per bucket.
+//
+// The reference offers, for a point at bucket position q, the other members
+// in position order (0..q-1 from the outer loop, then q+1..b-1 from its own
+// inner loop), each offer gated by dist < bound and applied with
+// KnnSetScannableSimd::addCandidateLessThan.  This kernel keeps that order
+// exactly: for a block of 64 points (4 per warp, sets held in registers) it
+// walks the bucket in 64-point column blocks in ascending order, computes the
+// 64x64 distance block in the reference's FP32 order from dim-major shared
+// memory tiles, then each warp replays its points' 64 offers in column order
+// (set_offer_batch).  Distances are computed for the full b x b matrix (both
+// triangles); each (i, j) and (j, i) evaluation gives the same bits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "context.hpp"
+#include "dispatch.hpp"
+
+namespace knng {
+namespace {
+
+constexpr int kLeafThreads = 512;
+constexpr int kLeafWarps = kLeafThreads / kWarp;  // 16
+constexpr int kBI = 64;                            // points updated per row block
+constexpr int kBJ = 64;                            // candidates per column block
+constexpr int kPtsPerWarp = kBI / kLeafWarps;      // 4
+constexpr int kJPerThread = kBI * kBJ / kLeafThreads;  // 8
+constexpr int kDmStride = kBJ + 1;
+
+// rows [base, base+64) of the bucket -> tile[dim][r] (zeros past the bucket end)
+template <int D>
+__device__ __forceinline__ void load_tile(float* __restrict__ tile, const uint32_t* __restrict__ ids, uint32_t base,
+                                          uint32_t b, const float* __restrict__ pts, int ld) {
+    constexpr int Q = D / 4;
+    for (int f = threadIdx.x; f < kBI * Q; f += kLeafThreads) {
+        const int r = f % kBI, q = f / kBI;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (base + r < b) v = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[base + r]) * ld) + q);
+        tile[(4 * q + 0) * kBI + r] = v.x;
+        tile[(4 * q + 1) * kBI + r] = v.y;
+        tile[(4 * q + 2) * kBI + r] = v.z;
+        tile[(4 * q + 3) * kBI + r] = v.w;
+    }
+}
+
+// Dm[i][j] = canonical distance(I row i, J row j), thread -> (i, 8 columns).
+template <int D>
+__device__ __forceinline__ void distance_block(const float* __restrict__ I, const float* __restrict__ J,
+                                               float* __restrict__ Dm) {
+    constexpr int M = D / 8 * 8;
+    const int i = threadIdx.x % kBI;
+    const int jg = threadIdx.x / kBI;  // 0..7
+    const float4* J4 = reinterpret_cast<const float4*>(J);
+    float tot[kJPerThread];
+#pragma unroll
+    for (int q = 0; q < kJPerThread; ++q) tot[q] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        float ch[kJPerThread];
+#pragma unroll
+        for (int q = 0; q < kJPerThread; ++q) ch[q] = 0.0f;
+#pragma unroll
+        for (int dim = c; dim < M; dim += 8) {
+            const float a = I[dim * kBI + i];
+            const float4 v0 = J4[dim * (kBJ / 4) + jg * 2 + 0];
+            const float4 v1 = J4[dim * (kBJ / 4) + jg * 2 + 1];
+            const float bv[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+            for (int q = 0; q < kJPerThread; ++q) {
+                const float diff = __fsub_rn(a, bv[q]);
+                ch[q] = __fmaf_rn(diff, diff, ch[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kJPerThread; ++q) tot[q] = __fadd_rn(tot[q], ch[q]);
+    }
+#pragma unroll
+    for (int dim = M; dim < D; ++dim) {
+        const float a = I[dim * kBI + i];
+        const float4 v0 = J4[dim * (kBJ / 4) + jg * 2 + 0];
+        const float4 v1 = J4[dim * (kBJ / 4) + jg * 2 + 1];
+        const float bv[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+        for (int q = 0; q < kJPerThread; ++q) {
+            const float diff = __fsub_rn(a, bv[q]);
+            tot[q] = __fadd_rn(tot[q], __fmul_rn(diff, diff));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kJPerThread; ++q) Dm[i * kDmStride + jg * kJPerThread + q] = tot[q];
+}
+
+template <int D>
+__global__ void __launch_bounds__(kLeafThreads, 1)
+    k_leaf(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends, const uint32_t* __restrict__ idx,
+           const float* __restrict__ pts, int ld, float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
+           uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound,
+           int K) {
+    extern __shared__ float4 smem4[];
+    float* I = reinterpret_cast<float*>(smem4);
+    float* J = I + D * kBI;
+    float* Dm = J + D * kBJ;
+    uint32_t* ids = reinterpret_cast<uint32_t*>(Dm + kBI * kDmStride);
+    const uint32_t s = starts[blockIdx.x];
+    const uint32_t b = ends[blockIdx.x] - s;
+    if (b < 2) return;
+    for (uint32_t t = threadIdx.x; t < b; t += kLeafThreads) ids[t] = idx[s + t];
+    __syncthreads();
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    for (uint32_t ib = 0; ib < b; ib += kBI) {
+        load_tile<D>(I, ids, ib, b, pts, ld);
+        WarpSet sets[kPtsPerWarp];
+#pragma unroll
+        for (int u = 0; u < kPtsPerWarp; ++u) {
+            const uint32_t p = ib + warp * kPtsPerWarp + u;
+            if (p < b) set_load(sets[u], set_dist, set_id, set_size, set_maxslot, set_bound, ids[p], K, lane);
+        }
+        for (uint32_t jb = 0; jb < b; jb += kBJ) {
+            __syncthreads();  // previous block's readers of J / Dm are done; I is written
+            load_tile<D>(J, ids, jb, b, pts, ld);
+            __syncthreads();
+            distance_block<D>(I, J, Dm);
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < kPtsPerWarp; ++u) {
+                const int row = warp * kPtsPerWarp + u;
+                const uint32_t p = ib + row;
+                if (p < b) {
+#pragma unroll
+                    for (int h = 0; h < kBJ / kWarp; ++h) {
+                        const int jj = h * kWarp + lane;
+                        const uint32_t j = jb + jj;
+                        const bool valid = j < b && j != p;
+                        const float d = Dm[row * kDmStride + jj];
+                        const uint32_t cand = valid ? ids[j] : 0u;
+                        set_offer_batch(sets[u], cand, d, valid, K, lane);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kPtsPerWarp; ++u) {
+            const uint32_t p = ib + warp * kPtsPerWarp + u;
+            if (p < b) set_store(sets[u], set_dist, set_id, set_size, set_maxslot, set_bound, ids[p], K, lane);
+        }
+        __syncthreads();  // everyone is done with I before it is reloaded
+    }
+}
+
+}  // namespace
+
+void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
+                   uint32_t max_bucket, uint64_t* evals) {
+    if (count == 0) return;
+    KNNG_DISPATCH_D(c.d, {
+        const size_t smem = static_cast<size_t>(D) * (kBI + kBJ) * sizeof(float) +
+                            static_cast<size_t>(kBI) * kDmStride * sizeof(float) +
+                            static_cast<size_t>(std::max<uint32_t>(max_bucket, 1)) * sizeof(uint32_t);
+        if (smem > 227 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "bucket too large for the bucket kernel");
+        auto kern = k_leaf<D>;
+        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        kern<<<count, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
+                                                      c.set_id, c.set_size, c.set_maxslot, c.set_bound,
+                                                      static_cast<int>(c.k));
+    });
+    ++c.launches;
+    KNNG_CUDA(cudaGetLastError());
+    (void)evals;
+}
+
+}  // namespace knng

@@ -1,0 +1,60 @@
+"""CPU tests of the C ABI: the library builds, loads and exports every symbol
+include/knng.h declares; host-only entry points behave.  No kernel runs."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from sigmod23ann_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols() -> list[str]:
+    names = []
+    for h in ("knng.h",):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(knng_[a-z_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_header_and_binding_agree():
+    assert declared_symbols() == sorted(api.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol(knng_lib):
+    for name in declared_symbols():
+        assert hasattr(knng_lib, name), name
+
+
+def test_default_params_are_the_references(knng_lib):
+    p = api.default_params()
+    assert (p.k, p.max_leaf, p.max_leaf_odd, p.lloyd_iters, p.small_threshold, p.seed) == (100, 200, 400, 1, 3000,
+                                                                                            12345)
+    assert p.refine == 1 and p.precision == api.PRECISION_FP32
+
+
+def test_status_strings(knng_lib):
+    for code in range(8):
+        assert knng_lib.knng_status_string(code)
+    assert knng_lib.knng_status_string(0) == b"ok"
+
+
+def test_struct_layouts_match_header():
+    # knng_params: 8 x uint32 + uint64; knng_stats: 6 doubles + 11 uint64.
+    assert ctypes.sizeof(api.Params) == 40
+    assert ctypes.sizeof(api.Stats) == 6 * 8 + 11 * 8
+
+
+def test_create_without_device_reports_no_device(knng_lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.KnngError) as e:
+        api.KnngContext(0)
+    assert e.value.status == 7

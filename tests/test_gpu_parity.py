@@ -1,0 +1,231 @@
+"""GPU parity tests: the CUDA library, called through the C ABI, against the
+oracle (and, through the golden fixtures, against the reference's own code).
+
+Bar: bit-exact index permutations, set states (distance bits, ids, sizes,
+max slots, bounds) and final ids, given the same hyperplanes and buckets."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import assert_sets_equal, digest, feed_trace, sets_digest
+from sigmod23ann_b200 import KnngContext, KnngError, default_params, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(knng_lib):
+    c = KnngContext(0)
+    yield c
+    c.close()
+
+
+def oracle_rep_and_feed(oracle_lib, ctx, pts, reps, k=100, check_each=True):
+    """Runs the oracle with the reference RNG, then drives the GPU with the
+    oracle's hyperplanes and buckets; returns (oracle, per-rep checks)."""
+    o = oracle_lib.Oracle(pts, k=k, rng_mode=0, seed=12345)
+    ctx.load_points(pts)
+    ctx.reset_sets(k)
+    for r, (iters, leaf) in enumerate(reps):
+        o.rep(iters, leaf, r)
+        t = o.trace()
+        ctx.begin_rep()
+        feed_trace(ctx, t)
+        np.testing.assert_array_equal(ctx.indices(), o.indices())
+        ctx.process_leaves(t["leaf_start"], t["leaf_end"])
+        if check_each:
+            assert_sets_equal(ctx.sets(), o.sets(), f"rep {r}")
+    return o
+
+
+def test_golden_cases_through_gpu(oracle_lib, ctx, golden):
+    """Reference outputs (fixtures) reproduced by the GPU fed the hyperplanes."""
+    for name, case in golden["cases"].items():
+        pts = workloads.gaussian_mixture(**case["generator"])
+        o = oracle_lib.Oracle(pts, k=100, rng_mode=0, seed=12345)
+        ctx.load_points(pts)
+        ctx.reset_sets(100)
+        for r, (iters, leaf) in enumerate(case["reps"]):
+            o.rep(iters, leaf, r)
+            t = o.trace()
+            ctx.begin_rep()
+            feed_trace(ctx, t)
+            assert digest(ctx.indices()) == case["indices"][r], f"{name} rep {r} indices"
+            ctx.process_leaves(t["leaf_start"], t["leaf_end"])
+            assert sets_digest(ctx.sets()) == case["sets"][r], f"{name} rep {r} sets"
+        if case["topup"]:
+            assert ctx.refine() == case["topup_changed"]
+            assert sets_digest(ctx.sets()) == case["topup_sets"], f"{name} top-up"
+        assert digest(ctx.finalize()) == case["final"], f"{name} final"
+
+
+def test_split_leaf_parity_config1_shape(oracle_lib, ctx):
+    """20k points of the 64-Gaussian config-1 distribution, leaf <= 256, 2 Lloyd
+    iterations, 3 repetitions: every permutation and set state bit-exact."""
+    pts = workloads.gaussian_mixture(n=20_000, d=100, clusters=64, sigma=0.15, seed=0)
+    o = oracle_rep_and_feed(oracle_lib, ctx, pts, [(2, 257)] * 3)
+    ids, dist = ctx.finalize(want_dists=True)
+    oids, odist = o.finalize()
+    np.testing.assert_array_equal(ids, oids)
+    np.testing.assert_array_equal(dist.view(np.uint32), odist.view(np.uint32))
+
+
+def test_refine_parity(oracle_lib, ctx):
+    pts = workloads.gaussian_mixture(n=5000, d=100, clusters=16, sigma=0.2, seed=4)
+    o = oracle_rep_and_feed(oracle_lib, ctx, pts, [(1, 200), (1, 400)])
+    assert ctx.refine() == o.refine()
+    assert_sets_equal(ctx.sets(), o.sets(), "refine")
+
+
+def test_refine_parity_unfilled_sets(oracle_lib, ctx):
+    """Sets below k after tiny buckets: unfilled slots read as id 0 (quirk of
+    src/SolutionKmeans.hpp:494)."""
+    pts = workloads.gaussian_mixture(n=3000, d=100, clusters=8, sigma=0.2, seed=8)
+    o = oracle_rep_and_feed(oracle_lib, ctx, pts, [(1, 40)])
+    assert (o.sets()["size"] < 100).all()
+    assert ctx.refine() == o.refine()
+    assert_sets_equal(ctx.sets(), o.sets(), "refine unfilled")
+
+
+def test_farthest_pair_and_lloyd_parity(oracle_lib, ctx):
+    """Device seeding and Lloyd iterations from the oracle's seeds / samples
+    give the oracle's starting centres and hyperplanes."""
+    pts = workloads.gaussian_mixture(n=12_000, d=100, clusters=32, sigma=0.15, seed=6)
+    o = oracle_lib.Oracle(pts, k=100, rng_mode=0, seed=12345)
+    o.rep(2, 300, 0)
+    t = o.trace()
+    # Replay the permutation each node saw: feed level by level, checking per level.
+    ctx.load_points(pts)
+    ctx.reset_sets(100)
+    ctx.begin_rep()
+    from helpers import trace_levels
+
+    for sel in trace_levels(t):
+        off = np.zeros(len(sel) + 1, np.uint64)
+        pos = []
+        for j, i in enumerate(sel):
+            p = t["start_pos"][int(t["start_off"][i]):int(t["start_off"][i + 1])]
+            pos.append(p)
+            off[j + 1] = off[j] + len(p)
+        first, second, ok = ctx.farthest_pair(off, np.concatenate(pos))
+        assert ok.all()
+        idx = ctx.indices()
+        for j, i in enumerate(sel):
+            c1 = pts[idx[pos[j][first[j]]]]
+            c2 = pts[idx[pos[j][second[j]]]]
+            np.testing.assert_array_equal(c1, t["c1_start"][i])
+            np.testing.assert_array_equal(c2, t["c2_start"][i])
+        lo = np.zeros(len(sel) + 1, np.uint64)
+        lpos = []
+        for j, i in enumerate(sel):
+            p = t["lloyd_pos"][int(t["lloyd_off"][i]):int(t["lloyd_off"][i + 1])]
+            lpos.append(p)
+            lo[j + 1] = lo[j] + len(p)
+        coefs, offs, ok = ctx.lloyd(t["start"][sel], t["end"][sel], lo,
+                                    np.concatenate(lpos) if lpos else np.zeros(0, np.uint32),
+                                    t["c1_start"][sel], t["c2_start"][sel], 2)
+        assert ok.all()
+        np.testing.assert_array_equal(coefs.view(np.uint32), t["coefs"][sel].view(np.uint32))
+        np.testing.assert_array_equal(offs.view(np.uint32), t["offset"][sel].view(np.uint32))
+        mids = ctx.split_nodes(t["start"][sel], t["end"][sel], coefs, offs)
+        np.testing.assert_array_equal(mids, t["mid"][sel])
+    np.testing.assert_array_equal(ctx.indices(), o.indices())
+
+
+def test_device_seeded_rep_matches_counter_oracle(oracle_lib, ctx):
+    """knng_run_rep (device RNG, device Lloyd, device partition, buckets) equals
+    the oracle driven by the same counter RNG."""
+    pts = workloads.gaussian_mixture(n=15_000, d=100, clusters=32, sigma=0.15, seed=12)
+    o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=777)
+    ctx.load_points(pts)
+    ctx.reset_sets(100)
+    for r, leaf in enumerate([257, 400]):
+        o.rep(2, leaf, r)
+        ctx.run_rep(leaf, 2, 3000, 777, r)
+        np.testing.assert_array_equal(ctx.indices(), o.indices())
+        s, e = ctx.leaves()
+        t = o.trace()
+        order = np.argsort(t["leaf_start"])
+        np.testing.assert_array_equal(s, t["leaf_start"][order])
+        np.testing.assert_array_equal(e, t["leaf_end"][order])
+        assert_sets_equal(ctx.sets(), o.sets(), f"device rep {r}")
+
+
+def test_build_end_to_end_matches_oracle(oracle_lib, ctx):
+    pts = workloads.gaussian_mixture(n=8000, d=100, clusters=16, sigma=0.15, seed=13)
+    p = default_params(reps=3, max_leaf=200, max_leaf_odd=400, lloyd_iters=2, refine=1, seed=4242)
+    ids, dist = ctx.build(pts, p, want_dists=True)
+    o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=4242)
+    for r in range(3):
+        o.rep(2, 400 if r % 2 else 200, r)
+    o.refine()
+    oids, odist = o.finalize()
+    np.testing.assert_array_equal(ids, oids)
+    np.testing.assert_array_equal(dist.view(np.uint32), odist.view(np.uint32))
+
+
+@pytest.mark.parametrize("d,k", [(64, 10), (128, 50), (100, 1), (64, 128)])
+def test_other_shapes(oracle_lib, ctx, d, k):
+    pts = workloads.gaussian_mixture(n=3100, d=d, clusters=8, sigma=0.2, seed=d + k)
+    p = default_params(k=k, reps=2, max_leaf=150, max_leaf_odd=0, lloyd_iters=1, refine=1, seed=5)
+    ids = ctx.build(pts, p)
+    o = oracle_lib.Oracle(pts, k=k, rng_mode=1, seed=5)
+    for r in range(2):
+        o.rep(1, 150, r)
+    o.refine()
+    np.testing.assert_array_equal(ids, o.finalize()[0])
+
+
+def test_edge_cases(oracle_lib, ctx):
+    # One point: no pairs, row padded with id 1.
+    ids = ctx.build(np.ones((1, 100), np.float32), default_params(reps=1, refine=1))
+    assert ids.shape == (1, 100) and (ids == 1).all()
+    # Fewer points than k: rows hold n-1 neighbours then padding.
+    pts = workloads.gaussian_mixture(n=37, d=100, clusters=2, seed=1)
+    ids = ctx.build(pts, default_params(reps=2, refine=1))
+    for i in range(37):
+        assert sorted(ids[i, :36].tolist()) == sorted(set(range(37)) - {i})
+        assert (ids[i, 36:] == 1).all()
+    # Identical points: the reference loops forever; here every split falls back
+    # to the index midpoint and every distance is 0.
+    pts = np.zeros((900, 100), np.float32)
+    ids, dist = ctx.build(pts, default_params(k=16, reps=1, max_leaf=100, max_leaf_odd=0, refine=0),
+                          want_dists=True)
+    assert (dist == 0).all()
+    o = oracle_lib.Oracle(pts, k=16, rng_mode=1, seed=12345)
+    o.rep(1, 100, 0)
+    np.testing.assert_array_equal(ids, o.finalize()[0])
+    # Buckets of size 1 and 2 through the stepwise API.
+    pts = workloads.gaussian_mixture(n=10, d=100, clusters=2, seed=2)
+    ctx.load_points(pts)
+    ctx.reset_sets(4)
+    ctx.process_leaves([0, 1, 3], [1, 3, 10])
+    o = oracle_lib.Oracle(pts, k=4)
+    o.process_leaves(np.array([0, 1, 3]), np.array([1, 3, 10]))
+    assert_sets_equal(ctx.sets(), o.sets(), "tiny buckets")
+
+
+def test_invalid_arguments(ctx):
+    with pytest.raises(KnngError) as e:
+        ctx.build(np.zeros((10, 99), np.float32))
+    assert e.value.status == 6
+    with pytest.raises(KnngError) as e:
+        ctx.build(np.zeros((10, 100), np.float32), default_params(k=0))
+    assert e.value.status == 6
+    ctx.load_points(np.zeros((10, 100), np.float32))
+    ctx.reset_sets(4)
+    with pytest.raises(KnngError) as e:
+        ctx.process_leaves([0, 5], [6, 10])
+    assert e.value.status == 1
+    with pytest.raises(KnngError) as e:
+        ctx.set_indices(np.zeros(10, np.uint32))
+    assert e.value.status == 1
+
+
+def test_budget_is_enforced(knng_lib):
+    c = KnngContext(0, hbm_budget_bytes=1 << 20)
+    with pytest.raises(KnngError) as e:
+        c.build(np.zeros((100_000, 100), np.float32))
+    assert e.value.status == 4
+    c.close()
