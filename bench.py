@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""k-NN graph build throughput on B200: points/s for the 10M x 100, k=100
+build at recall >= 0.94 against an FP64 exact oracle.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one whole graph build (every repetition of split + bucket pass,
+then finalize) of the 10,000,000-point, 100-d, 1,024-cluster Zipf(1.1)
+24-d-subspace mixture (seed 1), leaf buckets <= 1024, through the library's C
+ABI.  `value` is measured with the points already in HBM (knng_build_device),
+timed by CUDA events on the library's launching stream; `e2e` is the same
+build through knng_build with pinned host buffers, host<->device copies inside
+the timed region.  The input (4 GB) is larger than L2, so no flush is needed
+between steps.  With N > 1 (torchrun), every rank builds its own replica: the
+path has no exchange step, so scaling is weak and there is no collective on
+the data path; the step time is the maximum over ranks.
+
+--impl reference times the reference's own CPU code (oracle/_ref, the
+reference headers compiled against a std::thread-pool stand-in for TBB) on the
+host cores: each step is one repetition of splitKmeansBinaryProcess over a
+bounded prefix of the same point set, scaled to a whole build (value =
+points / (t_rep * reps)).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "points/sec k-NN graph build at recall>=0.94 (10M x 100, k=100); p50/p99 latency"
+N_POINTS = 10_000_000
+DIM = 100
+K = 100
+MAX_LEAF = 1025        # buckets of at most 1024 points (leaf iff size < max_leaf)
+LLOYD_ITERS = 2
+REPS = 6
+REFINE = 0
+SEED = 1
+QUERIES = 10_000
+FP32_NOMINAL_TFLOPS_AT_MAX_CLOCK = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_POINTS)
+    ap.add_argument("--reps", type=int, default=REPS)
+    ap.add_argument("--refine", type=int, default=REFINE)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work per reference sample")
+    return ap.parse_args(argv)
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def dist_done(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ reference arm
+
+def reference_sample_rate(points: np.ndarray, reps_per_build: int, target_s: float, steps: int, warmup: int):
+    """Times the reference's splitKmeansBinaryProcess (one repetition, leaf <= 1024,
+    2 Lloyd iterations) on a prefix of the point set with all host threads.
+    Returns per-step points/s scaled to a whole build, the sample size and cores."""
+    from oracle import bindings
+
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("KNNG_REF_THREADS", str(cores))
+    cores = int(os.environ["KNNG_REF_THREADS"])
+    if not bindings.reference_available():
+        return None
+    # Calibrate the prefix so one repetition takes about target_s seconds.
+    m = min(len(points), 100_000)
+    while True:
+        ref = bindings.ReferenceShim(points[:m], threaded=True)
+        t = time.perf_counter()
+        ref.rep(LLOYD_ITERS, MAX_LEAF)
+        dt = time.perf_counter() - t
+        ref.close()
+        if dt >= target_s / 3 or m >= len(points):
+            break
+        m = min(len(points), int(m * max(2.0, target_s / max(dt, 1e-3) * 0.8)))
+    ref = bindings.ReferenceShim(points[:m], threaded=True)
+    for _ in range(warmup):
+        ref.rep(LLOYD_ITERS, MAX_LEAF)
+    rates = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        ref.rep(LLOYD_ITERS, MAX_LEAF)
+        dt = time.perf_counter() - t
+        rates.append(m / (dt * reps_per_build))
+    ref.close()
+    return {"rates": rates, "sample_points": m, "cores": cores}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    try:
+        if rank != 0:
+            return 0
+        from sigmod23ann_b200 import workloads
+
+        pts = workloads.subspace_mixture(min(args.n, 2_000_000), seed=SEED)
+        res = reference_sample_rate(pts, args.reps, args.cpu_seconds, args.steps, args.warmup)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (needs the reference sources)"}))
+            return 0
+        value = statistics.mean(res["rates"])
+        sample = (f"one repetition of the reference splitKmeansBinaryProcess (leaf<=1024, {LLOYD_ITERS} Lloyd "
+                  f"iterations) on the first {res['sample_points']:,} points of the seed-1 subspace mixture, "
+                  f"scaled to a {args.reps}-repetition build")
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.n / value * 1000.0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "10M x 100 f32 subspace mixture, k=100, leaf<=1024 (sampled prefix on CPU)",
+                       "reps": args.reps, "lloyd_iters": LLOYD_ITERS},
+            "cpu_baseline": {"value": value, "unit": "points/s", "cores": res["cores"], "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return 0
+    finally:
+        dist_done(world)
+
+
+# ------------------------------------------------------------ our arm
+
+def run_ours(args):
+    import torch
+
+    from sigmod23ann_b200 import KnngContext, Stats, default_params, groundtruth, workloads
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    n = args.n
+    params = default_params(k=K, max_leaf=MAX_LEAF, max_leaf_odd=0, lloyd_iters=LLOYD_ITERS, reps=args.reps,
+                            refine=args.refine, seed=SEED)
+    x = workloads.subspace_mixture_torch(n, seed=SEED, device=f"cuda:{local}")
+    ids = torch.empty((n, K), dtype=torch.int32, device=f"cuda:{local}")
+    ctx = KnngContext(local)
+    for _ in range(args.warmup):
+        ctx.build_device(x.data_ptr(), n, DIM, ids.data_ptr(), None, params)
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    device_ms, leaf_ms, launches, leaf_launches, pairs, stats_list = 0.0, 0.0, 0, 0, 0, []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = Stats()
+        ctx.build_device(x.data_ptr(), n, DIM, ids.data_ptr(), None, params, stats=st)
+        device_ms += st.ms_total + st.ms_finalize
+        leaf_ms += st.ms_leaf_kernel
+        launches += st.kernel_launches
+        leaf_launches += st.leaf_launches
+        pairs += st.bucket_pairs
+        stats_list.append(st.as_dict())
+    ev1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clock = clocks.stop()
+    dist_barrier(world)
+    stream_ms = ev0.elapsed_time(ev1)
+    ms_step = dist_max(device_ms / args.steps, world)
+    value = world * n / (ms_step / 1000.0)
+
+    # Recall of the last build against the FP64 oracle on sampled points.
+    q = np.random.default_rng(SEED).choice(n, min(QUERIES, n), replace=False)
+    gt = groundtruth.exact_knn_torch(x, q, K)
+    rec = groundtruth.recall(ids.cpu().numpy().view(np.uint32), gt, q)
+
+    # End to end through the host-pointer ABI, pinned buffers.
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.empty((n, DIM), dtype=torch.float32, pin_memory=True)
+        host_in.copy_(x.cpu())
+        host_out = torch.empty((n, K), dtype=torch.int32, pin_memory=True)
+        del x, ids
+        torch.cuda.empty_cache()
+        hin, hout = host_in.numpy(), host_out.numpy().view(np.uint32)
+        lib = ctx._lib
+        import ctypes
+
+        from sigmod23ann_b200.api import _ptr
+
+        def one():
+            st = Stats()
+            ctx._check(lib.knng_build(ctx._h, _ptr(hin), n, DIM, DIM * 4, ctypes.byref(params), _ptr(hout), None,
+                                      ctypes.byref(st)))
+
+        one()
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        times = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            one()
+            times.append(time.perf_counter() - t)
+        e_ms = dist_max(1000.0 * statistics.mean(times), world)
+        e2e = {"value": world * n / (e_ms / 1000.0), "unit": "points/s", "h2d_bytes_per_step": n * DIM * 4,
+               "d2h_bytes_per_step": n * K * 4, "ms_per_step": e_ms}
+
+    line = None
+    if rank == 0:
+        per_launch_ms = leaf_ms / max(1, leaf_launches)
+        # Bucket kernel: the reference's unique-pair work, 3*d FLOPs per pair
+        # (d subtractions + d fused multiply-adds).
+        flops_per_launch = 3.0 * DIM * pairs / max(1, leaf_launches)
+        achieved = flops_per_launch / (per_launch_ms / 1000.0) / 1e12
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS_AT_MAX_CLOCK,
+                    "unit": "TFLOP/s", "frac": achieved / FP32_NOMINAL_TFLOPS_AT_MAX_CLOCK, "traffic": None,
+                    "kernel": "k_leaf (bucket all-pairs + set updates)",
+                    "peak_source": "nominal FP32 FMA rate, 148 SMs x 128 lanes x 2 x 1965 MHz (no measured FP32 peak)",
+                    "ms_per_launch": per_launch_ms, "share_of_step": leaf_ms / max(device_ms, 1e-9)}
+        line = {
+            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{n:,} x {DIM} f32, 1024-cluster Zipf(1.1) 24-d subspace mixture (seed {SEED}), "
+                                   f"k={K}, leaf<=1024, {args.reps} repetitions, {LLOYD_ITERS} Lloyd iterations, "
+                                   f"refine={args.refine}",
+                       "n": n, "k": K, "reps": args.reps, "parallelism": f"replicas x{world}",
+                       "l2": "input 4 GB > 126 MB L2; no flush between steps"},
+            "recall": rec, "recall_queries": len(q), "meets_recall_target": rec >= 0.94,
+            "clocks": clock, "gpu_launches": launches, "stream_ms_total": stream_ms, "wall_s": wall,
+            "roofline": roofline, "e2e": e2e,
+            "stats_last_step": stats_list[-1],
+        }
+    ctx.close()
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        try:
+            from sigmod23ann_b200 import workloads as wl
+
+            pts = wl.subspace_mixture(min(n, 2_000_000), seed=SEED)
+            res = reference_sample_rate(pts, args.reps, args.cpu_seconds, 1, 0)
+            if res:
+                line["cpu_baseline"] = {
+                    "value": res["rates"][0], "unit": "points/s", "cores": res["cores"], "kind": "reference",
+                    "sample": f"one repetition of the reference splitKmeansBinaryProcess on the first "
+                              f"{res['sample_points']:,} points (numpy copy of the same distribution), "
+                              f"scaled to a {args.reps}-repetition build"}
+        except Exception as e:  # the baseline must not hide the GPU number
+            line["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    dist_done(world)
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -63,7 +63,8 @@ typedef struct knng_params {
                                  alternation of src/SolutionKmeans.hpp:582-587); 0 = max_leaf */
     uint32_t lloyd_iters;     /* 2-means iterations per split (knnIterations, :591) */
     uint32_t reps;            /* repetitions of split + bucket pass (the loop at :579-602) */
-    uint32_t refine;          /* 1 = run the neighbour-of-neighbour pass (topUpSingle, :604) */
+    uint32_t refine;          /* neighbour-of-neighbour passes after the repetitions (topUpSingle,
+                                 :604; the reference runs 1) */
     uint32_t small_threshold; /* nodes below this size run Lloyd over all their points (:156, 3000) */
     uint32_t precision;       /* KNNG_PRECISION_* */
     uint64_t seed;            /* keys the device's counter-based RNG */
@@ -88,6 +89,15 @@ typedef struct knng_stats {
     uint64_t leaf_launches;   /* bucket-kernel launches */
     uint64_t kernel_launches; /* all kernels launched by the call */
     uint64_t refine_changed;  /* points whose set changed in the refinement pass */
+    double ms_refine_join;    /* refinement: reverse lists + tensor-core join */
+    double ms_refine_apply;   /* refinement: sorted replay of survivors */
+    double ms_refine_fallback;/* refinement: unused by the join (0) */
+    uint64_t refine_pairs;    /* (point, candidate) pairs the join evaluated */
+    uint64_t refine_filter_pass; /* pairs the tensor-core bound could not reject */
+    uint64_t refine_member_skip; /* of those, candidates already in the point's list */
+    uint64_t refine_exact;    /* exact FP32 distances computed by the join */
+    uint64_t refine_emits;    /* survivor records written (before de-duplication) */
+    uint64_t refine_overflow; /* store rounds the join needed (survivor memory cap) */
 } knng_stats;
 
 /* Fills the reference's parameters: k=100, max_leaf=200, max_leaf_odd=400,
@@ -173,8 +183,9 @@ knng_status knng_get_leaves(knng_context* ctx, uint32_t capacity, uint32_t* star
                             uint32_t* out_count);
 
 /* Neighbour-of-neighbour pass (topUpSingle, src/SolutionKmeans.hpp:480-555),
- * candidates offered in ascending id order.  out_changed may be NULL. */
-knng_status knng_refine(knng_context* ctx, uint64_t* out_changed);
+ * candidates offered in ascending id order.  out_changed and stats (its
+ * refinement fields are added to) may be NULL. */
+knng_status knng_refine(knng_context* ctx, uint64_t* out_changed, knng_stats* stats);
 
 knng_status knng_get_indices(knng_context* ctx, uint32_t* out);
 knng_status knng_set_indices(knng_context* ctx, const uint32_t* in);
@@ -190,6 +201,14 @@ knng_status knng_set_sets(knng_context* ctx, const float* dist, const uint32_t* 
 /* Sorted, padded output (finalize + padResult, src/KnnSets.hpp:113-126,
  * :334-344): out_ids n*k, out_dists n*k (may be NULL). Host pointers. */
 knng_status knng_finalize(knng_context* ctx, uint32_t* out_ids, float* out_dists);
+
+/* -------------------------------------------------------------- diagnostics
+ * No counterpart in the reference.  Runs one 128 x 128 tensor-core tile
+ * (tcgen05.mma kind::tf32, the tile the refinement pass filters with) on
+ * a (m x d) and b (n x d), m, n <= 128, writing out[i*n + j] = a_i . b_j
+ * with TF32 operands and FP32 accumulation. */
+knng_status knng_debug_tile_gram(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n,
+                                 uint32_t d, float* out);
 
 #ifdef __cplusplus
 }

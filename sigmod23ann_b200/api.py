@@ -32,6 +32,7 @@ EXPORTED = [
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
+    "knng_debug_tile_gram",
 ]
 
 
@@ -51,6 +52,9 @@ class Stats(Structure):
         ("fallback_splits", c_uint64), ("buckets", c_uint64), ("bucket_pairs", c_uint64),
         ("bucket_pair_evals", c_uint64), ("leaf_launches", c_uint64), ("kernel_launches", c_uint64),
         ("refine_changed", c_uint64),
+        ("ms_refine_join", c_double), ("ms_refine_apply", c_double), ("ms_refine_fallback", c_double),
+        ("refine_pairs", c_uint64), ("refine_filter_pass", c_uint64), ("refine_member_skip", c_uint64),
+        ("refine_exact", c_uint64), ("refine_emits", c_uint64), ("refine_overflow", c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -92,12 +96,13 @@ def load_library(path: str = LIB_PATH):
         "knng_process_leaves": (c_int, [P, c_uint32, P, P]),
         "knng_run_rep": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, c_uint32, POINTER(Stats)]),
         "knng_get_leaves": (c_int, [P, c_uint32, P, P, P]),
-        "knng_refine": (c_int, [P, P]),
+        "knng_refine": (c_int, [P, P, POINTER(Stats)]),
         "knng_get_indices": (c_int, [P, P]),
         "knng_set_indices": (c_int, [P, P]),
         "knng_get_sets": (c_int, [P, P, P, P, P, P]),
         "knng_set_sets": (c_int, [P, P, P, P, P, P]),
         "knng_finalize": (c_int, [P, P, P]),
+        "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -262,9 +267,9 @@ class KnngContext:
         self._check(self._lib.knng_get_leaves(self._h, cnt.value, _ptr(s), _ptr(e), ctypes.byref(cnt)))
         return s, e
 
-    def refine(self) -> int:
+    def refine(self, stats: Stats | None = None) -> int:
         out = np.zeros(1, np.uint64)
-        self._check(self._lib.knng_refine(self._h, _ptr(out)))
+        self._check(self._lib.knng_refine(self._h, _ptr(out), ctypes.byref(stats) if stats is not None else None))
         return int(out[0])
 
     def indices(self) -> np.ndarray:
@@ -295,6 +300,15 @@ class KnngContext:
         dists = np.zeros((self.n, self.k), np.float32) if want_dists else None
         self._check(self._lib.knng_finalize(self._h, _ptr(ids), _ptr(dists)))
         return (ids, dists) if want_dists else ids
+
+
+def debug_tile_gram(ctx: "KnngContext", a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """a . b^T through one tcgen05 TF32 tile (diagnostic)."""
+    a = _f32(a)
+    b = _f32(b)
+    out = np.zeros((a.shape[0], b.shape[0]), np.float32)
+    ctx._check(ctx._lib.knng_debug_tile_gram(ctx._h, _ptr(a), a.shape[0], _ptr(b), b.shape[0], a.shape[1], _ptr(out)))
+    return out
 
 
 def construct_result(points: np.ndarray, params: Params | None = None, device: int = 0) -> np.ndarray:

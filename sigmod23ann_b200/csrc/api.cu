@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -408,6 +409,21 @@ void add_rep_stats(knng_stats* s, const RepStats& st) {
     s->ms_leaf += st.ms_leaf;
 }
 
+void add_refine_stats(knng_stats* stats, const Context& c, uint64_t changed, double ms) {
+    if (!stats) return;
+    stats->ms_refine += ms;
+    stats->refine_changed += changed;
+    stats->ms_refine_join += c.last_refine.ms_join;
+    stats->ms_refine_apply += c.last_refine.ms_apply;
+    stats->ms_refine_fallback += c.last_refine.ms_fallback;
+    stats->refine_pairs += c.last_refine.pairs;
+    stats->refine_filter_pass += c.last_refine.filter_pass;
+    stats->refine_member_skip += c.last_refine.member_skip;
+    stats->refine_exact += c.last_refine.exact;
+    stats->refine_emits += c.last_refine.emits;
+    stats->refine_overflow += c.last_refine.overflow;
+}
+
 void validate_params(const knng_params* p) {
     if (!p) fail(KNNG_ERR_INVALID_ARGUMENT, "params is null");
     if (p->k == 0 || p->k > static_cast<uint32_t>(kMaxK)) fail(KNNG_ERR_UNSUPPORTED, "k must be in 1..128");
@@ -428,14 +444,10 @@ void build_all(Context& c, const knng_params* p, knng_stats* stats) {
         add_rep_stats(stats, st);
         if (stats) stats->reps_done += 1;
     }
-    if (p->refine) {
+    for (uint32_t pass = 0; pass < p->refine; ++pass) {
         EventPair rt(c);
         const uint64_t ch = run_refine(c);
-        const double ms = rt.stop(c);
-        if (stats) {
-            stats->ms_refine += ms;
-            stats->refine_changed += ch;
-        }
+        add_refine_stats(stats, c, ch, rt.stop(c));
     }
     const double ms = total_t.stop(c);
     if (stats) {
@@ -515,6 +527,7 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     auto* c = new (std::nothrow) Context();
     if (!c) return KNNG_ERR_OUT_OF_MEMORY;
     c->device = device;
+    if (const char* r = std::getenv("KNNG_REFINE")) c->refine_mode = std::strcmp(r, "pointwise") == 0 ? 1 : 0;
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
@@ -702,11 +715,14 @@ knng_status knng_get_leaves(knng_context* ctx, uint32_t capacity, uint32_t* star
     });
 }
 
-knng_status knng_refine(knng_context* ctx, uint64_t* out_changed) {
+knng_status knng_refine(knng_context* ctx, uint64_t* out_changed, knng_stats* stats) {
     return knng::guarded(ctx, [&](Context& c) {
         knng::require_sets(c);
+        knng::EventPair t(c);
         const uint64_t ch = knng::run_refine(c);
+        const double ms = t.stop(c);
         if (out_changed) *out_changed = ch;
+        knng::add_refine_stats(stats, c, ch, ms);
     });
 }
 
@@ -812,6 +828,20 @@ knng_status knng_build_device(knng_context* ctx, const float* d_points, uint32_t
             stats->kernel_launches += c.launches - l0;
         }
         KNNG_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+knng_status knng_debug_tile_gram(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n, uint32_t d,
+                                 float* out) {
+    return knng::guarded(ctx, [&](Context& c) {
+        if (!a || !b || !out) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null array");
+        if (m == 0 || n == 0 || m > 128 || n > 128) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "m and n must be in 1..128");
+        if (!knng::dim_supported(d)) knng::fail(KNNG_ERR_UNSUPPORTED, "dimension must be 64, 100 or 128");
+        float* da = knng::upload(c, "dbg_a", a, static_cast<size_t>(m) * d);
+        float* db = knng::upload(c, "dbg_b", b, static_cast<size_t>(n) * d);
+        float* dout = static_cast<float*>(knng::scratch(c, "dbg_out", static_cast<size_t>(m) * n * sizeof(float)));
+        knng::run_tile_gram(c, d, da, m, db, n, dout);
+        knng::download(c, out, dout, static_cast<size_t>(m) * n);
     });
 }
 

@@ -63,6 +63,15 @@ struct Context {
     std::vector<std::pair<std::string, DeviceBuffer>> scratch;
 
     uint64_t launches = 0;
+
+    // Neighbour-of-neighbour pass: 0 = local join on the tensor cores,
+    // 1 = one warp per point (environment KNNG_REFINE=pointwise at creation).
+    int refine_mode = 0;
+    // Breakdown of the last refinement pass.
+    struct RefineRecord {
+        double ms_join = 0, ms_apply = 0, ms_fallback = 0;
+        uint64_t pairs = 0, filter_pass = 0, member_skip = 0, exact = 0, emits = 0, overflow = 0;
+    } last_refine;
 };
 
 // Allocation helpers (budget-checked).
@@ -119,6 +128,8 @@ void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const u
                    uint32_t max_bucket, uint64_t* evals);
 // refine.cu
 uint64_t run_refine(Context& c);
+// One tensor-core tile a(m x d) . b(n x d)^T into d_out (m x n), m, n <= 128.
+void run_tile_gram(Context& c, uint32_t d, const float* d_a, uint32_t m, const float* d_b, uint32_t n, float* d_out);
 // finalize.cu
 void launch_finalize(Context& c, uint32_t* d_ids, float* d_dists);
 void launch_reset_sets(Context& c);

@@ -21,12 +21,31 @@
 #include "common.cuh"
 #include "context.hpp"
 #include "dispatch.hpp"
+#include "tc.cuh"
 
 namespace knng {
 namespace {
 
-constexpr int kRefWarps = 8;
-constexpr int kSurvCap = 512;
+constexpr int kSnapWarps = 8;
+constexpr int kRefWarps = 4;
+constexpr int kSurvCap = 256;
+
+constexpr int kSeenSlots = 2048;  // per-warp open-addressing set of candidate ids
+constexpr int kSeenProbes = 32;
+
+// Inserts id into the warp's seen-set; true if it was not there.  When the
+// probe limit is reached the id is reported new: a repeated offer is harmless
+// (the set update rejects it), only slower.
+__device__ __forceinline__ bool seen_insert(uint32_t* seen, uint32_t id) {
+    uint32_t h = (id * 0x9E3779B1u) >> (32 - 11);
+    for (int probe = 0; probe < kSeenProbes; ++probe) {
+        const uint32_t prev = atomicCAS(&seen[h], kNone, id);
+        if (prev == kNone) return true;
+        if (prev == id) return false;
+        h = (h + 1) & (kSeenSlots - 1);
+    }
+    return true;
+}
 
 __host__ __device__ uint32_t pow2_at_least(uint32_t v) {
     uint32_t p = 2;
@@ -34,12 +53,12 @@ __host__ __device__ uint32_t pow2_at_least(uint32_t v) {
     return p;
 }
 
-__global__ void __launch_bounds__(kRefWarps * kWarp) k_snapshot(const uint32_t* __restrict__ set_id, uint32_t n, int K,
-                                                                uint32_t* __restrict__ snap) {
-    __shared__ unsigned long long keys_s[kRefWarps][kMaxK];
+__global__ void __launch_bounds__(kSnapWarps * kWarp) k_snapshot(const uint32_t* __restrict__ set_id, uint32_t n, int K,
+                                                                 uint32_t* __restrict__ snap) {
+    __shared__ unsigned long long keys_s[kSnapWarps][kMaxK];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     unsigned long long* keys = keys_s[warp];
-    for (uint32_t p = blockIdx.x * kRefWarps + warp; p < n; p += gridDim.x * kRefWarps) {
+    for (uint32_t p = blockIdx.x * kSnapWarps + warp; p < n; p += gridDim.x * kSnapWarps) {
         const size_t base = static_cast<size_t>(p) * K;
         for (int slot = lane; slot < kMaxK; slot += kWarp) keys[slot] = slot < K ? set_id[base + slot] : ~0ull;
         __syncwarp();
@@ -53,21 +72,34 @@ template <int D>
 __global__ void __launch_bounds__(kRefWarps * kWarp)
     k_refine(const uint32_t* __restrict__ snap, const float* __restrict__ pts, int ld, float* __restrict__ set_dist,
              uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
-             float* __restrict__ set_bound, int K, uint32_t n, unsigned long long* __restrict__ scratch_keys,
-             uint32_t warp_capacity, uint32_t* __restrict__ changed_count) {
+             float* __restrict__ set_bound, int K, uint32_t n, const uint32_t* __restrict__ plist,
+             unsigned long long* __restrict__ scratch_keys, uint32_t warp_capacity,
+             uint32_t* __restrict__ changed_count) {
     constexpr int Q = D / 4;
     __shared__ float4 rowp_s[kRefWarps][Q];
     __shared__ unsigned long long surv_s[kRefWarps][kSurvCap];
+    __shared__ uint32_t seen_s[kRefWarps][kSeenSlots];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     const uint32_t gw = blockIdx.x * kRefWarps + warp;
     const uint32_t nw = gridDim.x * kRefWarps;
     unsigned long long* gbuf = scratch_keys + static_cast<size_t>(gw) * warp_capacity;
     const unsigned lt_mask = (1u << lane) - 1u;
-    for (uint32_t p = gw; p < n; p += nw) {
+    for (uint32_t w = gw; w < n; w += nw) {
+        const uint32_t p = plist ? plist[w] : w;
         for (int q = lane; q < Q; q += kWarp)
             rowp_s[warp][q] = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(p) * ld) + q);
         WarpSet s;
         set_load(s, set_dist, set_id, set_size, set_maxslot, set_bound, p, K, lane);
+        // Seen-set: p itself and p's current members are pre-inserted, so
+        // candidates that could only be rejected (self, already a member, or a
+        // repeat from another list) skip the row gather and the distance.
+        uint32_t* seen = seen_s[warp];
+        for (int t = lane; t < kSeenSlots; t += kWarp) seen[t] = kNone;
+        __syncwarp();
+        if (lane == 0) seen_insert(seen, p);
+#pragma unroll
+        for (int r = 0; r < kSlotsPerLane; ++r)
+            if (lane + r * kWarp < static_cast<int>(s.size)) seen_insert(seen, s.id[r]);
         __syncwarp();
         const float bound0 = s.bound;
         uint32_t S = 0;
@@ -81,7 +113,7 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
             for (int b0 = 0; b0 < K; b0 += kWarp) {
                 const int bb = b0 + lane;
                 const uint32_t c = bb < K ? theirs[bb] : p;
-                const bool valid = c != p;
+                const bool valid = c != p && seen_insert(seen, c);
                 float d = 0.0f;
                 if (valid)
                     d = canonical_distance4<D>(reinterpret_cast<const float4*>(pts + static_cast<size_t>(c) * ld),
@@ -120,32 +152,716 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
     }
 }
 
+// ------------------------------------------------------------ local join
+//
+// The same pass, reorganised around the shared point q: p's candidates are
+// the lists S(q) of every q in S(p), so for each q the block
+// R(q) x S(q) (R(q) = the points whose list holds q) carries every candidate
+// pair that goes through q.  Each block reads |R(q)| + |S(q)| rows instead of
+// one row per (p, candidate), and its dot products run on the tensor cores:
+//
+//   1. k_rev_count / scan / k_rev_fill   R(q) as a CSR (counting sort)
+//   2. k_join     per q: S(q) rows and 128-point chunks of R(q) rows, centred
+//                 on q, staged as TF32 tiles; one tcgen05 128x128 tile gives
+//                 approximate squared distances with a proven error bound, so
+//                 a pair is dropped only when its exact distance is certainly
+//                 >= bound(p).  Survivors are checked against S(p) (binary
+//                 search in shared memory: members are always rejected by the
+//                 set update), get the exact FP32 distance in the reference's
+//                 order, and when it beats bound(p) are appended to p's
+//                 survivor slots.
+//   3. k_apply    per p: survivors sorted by id, duplicates dropped, replayed
+//                 through the sequential set update in ascending id order --
+//                 the same offers, in the same order, as the per-point pass.
+//   Points whose survivors overflow their slots are redone by k_refine.
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const uint32_t* __restrict__ in, uint64_t n,
+                                                              unsigned long long* __restrict__ tile_sum) {
+    __shared__ unsigned long long ws[kScanThreads / kWarp];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
+    unsigned long long s = 0;
+#pragma unroll
+    for (int u = 0; u < kScanPer; ++u)
+        if (base + u < n) s += in[base + u];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if (threadIdx.x % kWarp == 0) ws[threadIdx.x / kWarp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kScanThreads / kWarp; ++w) t += ws[w];
+        tile_sum[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the tile sums in place (one CTA).
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(unsigned long long* __restrict__ tile_sum, uint32_t nt) {
+    __shared__ unsigned long long part[kScanThreads];
+    const uint32_t per = (nt + kScanThreads - 1) / kScanThreads;
+    const uint32_t b = threadIdx.x * per, e = min(nt, b + per);
+    unsigned long long s = 0;
+    for (uint32_t i = b; i < e; ++i) s += tile_sum[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long run = 0;
+        for (int t = 0; t < kScanThreads; ++t) {
+            const unsigned long long v = part[t];
+            part[t] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    unsigned long long run = part[threadIdx.x];
+    for (uint32_t i = b; i < e; ++i) {
+        const unsigned long long v = tile_sum[i];
+        tile_sum[i] = run;
+        run += v;
+    }
+}
+
+// out[i] = sum of in[0..i); out[n] = total.
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t* __restrict__ in, uint64_t n,
+                                                             const unsigned long long* __restrict__ tile_off,
+                                                             unsigned long long* __restrict__ out) {
+    __shared__ unsigned long long ws[kScanThreads / kWarp];
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
+    uint32_t v[kScanPer];
+    unsigned long long mine = 0;
+#pragma unroll
+    for (int u = 0; u < kScanPer; ++u) {
+        v[u] = base + u < n ? in[base + u] : 0u;
+        mine += v[u];
+    }
+    unsigned long long incl = mine;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == kWarp - 1) ws[warp] = incl;
+    __syncthreads();
+    unsigned long long wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += ws[w];
+    unsigned long long run = tile_off[blockIdx.x] + wbase + incl - mine;
+#pragma unroll
+    for (int u = 0; u < kScanPer; ++u) {
+        if (base + u < n) out[base + u] = run;
+        run += v[u];
+        if (base + u + 1 == n) out[n] = run;
+    }
+}
+
+// One warp per point p: every distinct q of S(p) counts / receives p.
+__global__ void k_rev_count(const uint32_t* __restrict__ snap, uint32_t n, int K, uint32_t* __restrict__ cnt) {
+    const int lane = threadIdx.x % kWarp;
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < n; p += gridDim.x * blockDim.x / kWarp) {
+        const uint32_t* row = snap + static_cast<size_t>(p) * K;
+        for (int a = lane; a < K; a += kWarp) {
+            const uint32_t q = row[a];
+            if (a == 0 || row[a - 1] != q) atomicAdd(&cnt[q], 1u);
+        }
+    }
+}
+
+__global__ void k_rev_fill(const uint32_t* __restrict__ snap, uint32_t n, int K,
+                           const unsigned long long* __restrict__ off, uint32_t* __restrict__ cursor,
+                           uint32_t* __restrict__ rev) {
+    const int lane = threadIdx.x % kWarp;
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < n; p += gridDim.x * blockDim.x / kWarp) {
+        const uint32_t* row = snap + static_cast<size_t>(p) * K;
+        for (int a = lane; a < K; a += kWarp) {
+            const uint32_t q = row[a];
+            if (a == 0 || row[a - 1] != q) rev[off[q] + atomicAdd(&cursor[q], 1u)] = p;
+        }
+    }
+}
+
+constexpr int kJoinThreads = 256;
+constexpr int kTile = 128;  // MMA M = N = 128
+
+template <int D>
+struct JoinLayout {
+    static constexpr int KP = (D + 7) / 8 * 8;  // K padded to the MMA step (8 tf32)
+    static constexpr int CH = KP / 4;           // 16-byte chunks per row
+    static constexpr size_t tile_bytes = static_cast<size_t>(kTile) * KP * 4;
+    // A', B' (centred TF32 tiles), original B rows, member masks, per-row scalars.
+    static constexpr size_t orig_bytes = static_cast<size_t>(kTile) * D * 4;
+    static constexpr size_t bytes = 2 * tile_bytes + orig_bytes + kTile * 4 * 4 + 5 * kTile * 4 + 128 * 4;
+};
+
+// rows[r] (r < count, else zeros) minus `centre`, into a chunk-major tile.
+template <int D>
+__device__ __forceinline__ void stage_centred(float* __restrict__ tile, const uint32_t* __restrict__ ids,
+                                              uint32_t count, const float* __restrict__ pts, int ld,
+                                              const float* __restrict__ centre) {
+    constexpr int CH = JoinLayout<D>::CH;
+    for (int f = threadIdx.x; f < kTile * CH; f += kJoinThreads) {
+        const int r = f % kTile, ch = f / kTile;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
+            const float4 x = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + ch);
+            const float4 m = reinterpret_cast<const float4*>(centre)[ch];
+            v = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z), __fsub_rn(x.w, m.w));
+        }
+        *reinterpret_cast<float4*>(reinterpret_cast<unsigned char*>(tile) + tc::chunk_offset(r, 4 * ch, kTile)) = v;
+    }
+}
+
+// Squared norm of row r of a chunk-major tile (any order: only feeds the bound).
+template <int D>
+__device__ __forceinline__ float tile_norm(const float* __restrict__ tile, int r) {
+    constexpr int CH = JoinLayout<D>::CH;
+    float s = 0.f;
+#pragma unroll 4
+    for (int ch = 0; ch < CH; ++ch) {
+        const float4 v = *reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(tile) +
+                                                          tc::chunk_offset(r, 4 * ch, kTile));
+        s = fmaf(v.x, v.x, fmaf(v.y, v.y, fmaf(v.z, v.z, fmaf(v.w, v.w, s))));
+    }
+    return s;
+}
+
+// Copies rows ids[r] (r < count) into a row-major tile of D floats per row.
+template <int D>
+__device__ __forceinline__ void stage_rows(float* __restrict__ dst, const uint32_t* __restrict__ ids, uint32_t count,
+                                           const float* __restrict__ pts, int ld) {
+    constexpr int Q = D / 4;
+    for (uint32_t f = threadIdx.x; f < count * Q; f += kJoinThreads) {
+        const uint32_t r = f / Q, q = f % Q;
+        reinterpret_cast<float4*>(dst)[f] =
+            __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + q);
+    }
+}
+
+// mode 0 counts survivors per point into surv_count; mode 1 writes them at
+// surv[surv_off[p] - base + cursor] for points p in [p_lo, p_hi).
+template <int D>
+__global__ void __launch_bounds__(kJoinThreads, 1)
+    k_join(const uint32_t* __restrict__ snap, const unsigned long long* __restrict__ rev_off,
+           const uint32_t* __restrict__ rev, const float* __restrict__ pts, int ld, const float* __restrict__ bound,
+           const uint32_t* __restrict__ set_size, int K, uint32_t n, int mode, uint32_t p_lo, uint32_t p_hi,
+           uint32_t* __restrict__ surv_count, const unsigned long long* __restrict__ surv_off,
+           unsigned long long surv_base, uint32_t* __restrict__ surv_fill, unsigned long long* __restrict__ surv,
+           uint32_t* __restrict__ error_flag, unsigned long long* __restrict__ counters) {
+    using L = JoinLayout<D>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* A = reinterpret_cast<float*>(smem);
+    float* B = reinterpret_cast<float*>(smem + L::tile_bytes);
+    float* Borig = reinterpret_cast<float*>(smem + 2 * L::tile_bytes);
+    uint32_t* masks = reinterpret_cast<uint32_t*>(smem + 2 * L::tile_bytes + L::orig_bytes);
+    float* normA = reinterpret_cast<float*>(masks + kTile * 4);
+    float* normB = normA + kTile;
+    float* bnd = normB + kTile;
+    uint32_t* pid = reinterpret_cast<uint32_t*>(bnd + kTile);
+    uint32_t* cid = pid + kTile;
+    float* centre = reinterpret_cast<float*>(cid + kTile);
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ uint32_t ncols_s;
+    const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
+    if (tid == 0) {
+        tc::mbar_init(&mbar, 1);
+        tc::fence_barrier_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = tc::idesc_tf32(kTile, kTile);
+    uint32_t phase = 0;
+    bool healthy = true;
+    unsigned long long n_pairs = 0, n_pass = 0, n_member = 0, n_exact = 0, n_emit = 0;
+    const int quarter = warp % 4, half = warp / 4;
+    const int row = quarter * kWarp + lane;  // TMEM lane / tile row of this thread
+    for (uint32_t q = blockIdx.x; q < n && healthy; q += gridDim.x) {
+        const unsigned long long rb = rev_off[q], re = rev_off[q + 1];
+        if (rb == re) continue;
+        // Columns: the distinct ids of S(q), ascending.
+        if (warp == 0) {
+            const uint32_t* sq = snap + static_cast<size_t>(q) * K;
+            uint32_t base = 0;
+            for (int a0 = 0; a0 < K; a0 += kWarp) {
+                const int a = a0 + lane;
+                const uint32_t v = a < K ? sq[a] : kNone;
+                const bool keep = a < K && (a == 0 || sq[a - 1] != v);
+                const unsigned m = __ballot_sync(kFull, keep);
+                if (keep) cid[base + __popc(m & ((1u << lane) - 1u))] = v;
+                base += __popc(m);
+            }
+            if (lane == 0) ncols_s = base;
+        }
+        for (int j = tid; j < D; j += kJoinThreads) centre[j] = pts[static_cast<size_t>(q) * ld + j];
+        __syncthreads();
+        const uint32_t nc = ncols_s;
+        stage_centred<D>(B, cid, nc, pts, ld, centre);
+        stage_rows<D>(Borig, cid, nc, pts, ld);
+        __syncthreads();
+        if (tid < kTile) normB[tid] = tile_norm<D>(B, tid);
+        for (unsigned long long cb = rb; cb < re && healthy; cb += kTile) {
+            const uint32_t m = static_cast<uint32_t>(min(static_cast<unsigned long long>(kTile), re - cb));
+            bool any = false;
+            if (tid < kTile) {
+                uint32_t p = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
+                if (p != kNone && (p < p_lo || p >= p_hi)) p = kNone;
+                pid[tid] = p;
+                bnd[tid] = p != kNone ? bound[p] : 0.0f;
+                any = p != kNone;
+            }
+            for (int t = tid; t < kTile * 4; t += kJoinThreads) masks[t] = 0u;
+            if (!__syncthreads_or(any)) continue;
+            stage_centred<D>(A, pid, m, pts, ld, centre);
+            // Member masks: bit j of row r set when column j is in S(pid[r]).
+            for (uint32_t f = tid; f < m * static_cast<uint32_t>(K); f += kJoinThreads) {
+                const uint32_t r = f / K, a = f % K;
+                const uint32_t p = pid[r];
+                if (p == kNone) continue;
+                const uint32_t v = snap[static_cast<size_t>(p) * K + a];
+                if (v == 0 && set_size[p] < static_cast<uint32_t>(K)) continue;  // empty slots read as id 0
+                int lo = 0, hi = static_cast<int>(nc);
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (cid[mid] < v) lo = mid + 1; else hi = mid;
+                }
+                if (lo < static_cast<int>(nc) && cid[lo] == v) atomicOr(&masks[r * 4 + (lo >> 5)], 1u << (lo & 31));
+            }
+            __syncthreads();
+            if (tid < kTile) normA[tid] = tile_norm<D>(A, tid);
+            tc::fence_proxy_async();
+            tc::fence_before_sync();
+            __syncthreads();
+            if (tid == 0) {
+                tc::fence_after_sync();
+                tc::issue_tile_tf32(tmem, tc::smem_u32(A), tc::smem_u32(B), kTile, kTile, L::KP, idesc);
+                tc::mma_commit(&mbar);
+            }
+            const bool done = tc::mbar_wait(&mbar, phase);
+            phase ^= 1u;
+            if (__syncthreads_or(!done)) {
+                if (tid == 0) atomicExch(error_flag, 1u);
+                healthy = false;
+                break;
+            }
+            tc::fence_after_sync();
+            const uint32_t p = row < static_cast<int>(m) ? pid[row] : kNone;
+            const float bp = row < static_cast<int>(m) ? bnd[row] : 0.0f;
+            const float na = normA[row];
+            const float4* prow = reinterpret_cast<const float4*>(pts + static_cast<size_t>(p == kNone ? 0 : p) * ld);
+#pragma unroll 1
+            for (int cc = 0; cc < 4; ++cc) {
+                const int j0 = half * 64 + cc * 16;
+                float g[16];
+                tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
+                tc::tmem_wait_ld();
+                if (p == kNone) continue;
+                // Tensor-core filter: bit u set when the pair may beat bound(p).
+                // |approx - exact| <= 2^-7 (|x'|^2 + |y'|^2) + 2^-16 |approx| covers the TF32
+                // operands, FP32 accumulation, centring and the reference's summation order.
+                uint32_t pass = 0;
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const float nb = normB[j0 + u];
+                    const float approx = na + nb - 2.0f * g[u];
+                    const float margin = 0.0078125f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + 1e-30f;
+                    if (j0 + u < static_cast<int>(nc) && approx - margin < bp) pass |= 1u << u;
+                }
+                n_pairs += static_cast<unsigned long long>(max(0, min(16, static_cast<int>(nc) - j0)));
+                n_pass += __popc(pass);
+                const uint32_t members = (masks[row * 4 + (j0 >> 5)] >> (j0 & 31)) & 0xFFFFu;
+                n_member += __popc(pass & members);
+                uint32_t todo = pass & ~members;
+#pragma unroll 1
+                while (todo) {
+                    const int u = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    const int j = j0 + u;
+                    const uint32_t c = cid[j];
+                    if (c == p) continue;
+                    ++n_exact;
+                    const float d = canonical_distance4<D>(reinterpret_cast<const float4*>(Borig + j * D), prow);
+                    if (d < bp) {
+                        ++n_emit;
+                        if (mode == 0) {
+                            atomicAdd(&surv_count[p], 1u);
+                        } else {
+                            const uint32_t slot = atomicAdd(&surv_fill[p], 1u);
+                            // The store pass repeats the counting pass exactly; the
+                            // guard keeps a disagreement from writing past p's range.
+                            if (slot < surv_count[p])
+                                surv[surv_off[p] - surv_base + slot] =
+                                    (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
+                            else
+                                atomicExch(error_flag, 2u);
+                        }
+                    }
+                }
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+        }
+    }
+    atomicAdd(&counters[0], n_pairs);
+    atomicAdd(&counters[1], n_pass);
+    atomicAdd(&counters[2], n_member);
+    atomicAdd(&counters[3], n_exact);
+    atomicAdd(&counters[4], n_emit);
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, kTile);
+    }
+}
+
+// Replays one point's survivors (buf[0..S), padded to P2 with ~0 and
+// sorted here) through the sequential set update in ascending id order.
+__device__ __forceinline__ uint32_t replay_sorted(unsigned long long* buf, uint32_t S, uint32_t P2, uint32_t p, int K,
+                                                  float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
+                                                  uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
+                                                  float* __restrict__ set_bound, int lane) {
+    __syncwarp();
+    warp_bitonic_sort(buf, P2, lane);
+    WarpSet s;
+    set_load(s, set_dist, set_id, set_size, set_maxslot, set_bound, p, K, lane);
+    uint32_t changed = 0;
+    for (uint32_t t0 = 0; t0 < S; t0 += kWarp) {
+        const uint32_t t = t0 + lane;
+        const unsigned long long key = t < S ? buf[t] : ~0ull;
+        const unsigned long long prev = (t > 0 && t < S) ? buf[t - 1] : ~0ull;
+        const uint32_t cid = static_cast<uint32_t>(key >> 32);
+        const float d = __uint_as_float(static_cast<uint32_t>(key & 0xFFFFFFFFu));
+        const bool valid = t < S && (t == 0 || static_cast<uint32_t>(prev >> 32) != cid);
+        changed += set_offer_batch(s, cid, d, valid, K, lane);
+    }
+    set_store(s, set_dist, set_id, set_size, set_maxslot, set_bound, p, K, lane);
+    __syncwarp();
+    return changed;
+}
+
+constexpr int kApplyCap = 1024;  // survivors sorted in shared memory per warp
+
+// Points in [p_lo, p_hi): survivors at surv[surv_off[p] - base ...], sorted in
+// shared memory when they fit; larger lists are queued on `big`.
+__global__ void __launch_bounds__(kRefWarps * kWarp)
+    k_apply(uint32_t p_lo, uint32_t p_hi, int K, const uint32_t* __restrict__ surv_count,
+            const unsigned long long* __restrict__ surv_off, unsigned long long surv_base,
+            const unsigned long long* __restrict__ surv, float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
+            uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound,
+            uint32_t* __restrict__ big, uint32_t* __restrict__ big_n, uint32_t* __restrict__ changed_count) {
+    __shared__ unsigned long long keys_s[kRefWarps][kApplyCap];
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    unsigned long long* buf = keys_s[warp];
+    for (uint32_t p = p_lo + blockIdx.x * kRefWarps + warp; p < p_hi; p += gridDim.x * kRefWarps) {
+        const uint32_t S = surv_count[p];
+        if (S == 0) continue;
+        if (S > kApplyCap) {
+            if (lane == 0) big[atomicAdd(big_n, 1u)] = p;
+            continue;
+        }
+        const uint32_t P2 = pow2_at_least(S);
+        const unsigned long long* src = surv + (surv_off[p] - surv_base);
+        for (uint32_t t = lane; t < P2; t += kWarp) buf[t] = t < S ? src[t] : ~0ull;
+        const uint32_t ch = replay_sorted(buf, S, P2, p, K, set_dist, set_id, set_size, set_maxslot, set_bound, lane);
+        if (ch && lane == 0) atomicAdd(changed_count, 1u);
+    }
+}
+
+// Queued points with more than kApplyCap survivors: sorted in a per-warp
+// global scratch region of `cap` (a power of two >= the largest list) entries.
+__global__ void __launch_bounds__(kRefWarps * kWarp)
+    k_apply_big(const uint32_t* __restrict__ big, const uint32_t* __restrict__ big_n, int K,
+                const uint32_t* __restrict__ surv_count, const unsigned long long* __restrict__ surv_off,
+                unsigned long long surv_base, const unsigned long long* __restrict__ surv,
+                unsigned long long* __restrict__ scratch_keys, uint32_t cap, float* __restrict__ set_dist,
+                uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
+                float* __restrict__ set_bound, uint32_t* __restrict__ changed_count) {
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    const uint32_t gw = blockIdx.x * kRefWarps + warp;
+    unsigned long long* buf = scratch_keys + static_cast<size_t>(gw) * cap;
+    const uint32_t total = *big_n;
+    for (uint32_t w = gw; w < total; w += gridDim.x * kRefWarps) {
+        const uint32_t p = big[w];
+        const uint32_t S = surv_count[p];
+        const uint32_t P2 = pow2_at_least(S);
+        const unsigned long long* src = surv + (surv_off[p] - surv_base);
+        for (uint32_t t = lane; t < P2; t += kWarp) buf[t] = t < S ? src[t] : ~0ull;
+        const uint32_t ch = replay_sorted(buf, S, P2, p, K, set_dist, set_id, set_size, set_maxslot, set_bound, lane);
+        if (ch && lane == 0) atomicAdd(changed_count, 1u);
+    }
+}
+
+// One 128 x 128 TF32 tile of a(m x D) . b(n x D)^T (rows past m / n are zero);
+// the diagnostic behind knng_debug_tile_gram.
+template <int D>
+__global__ void __launch_bounds__(kJoinThreads, 1)
+    k_tile_gram(const float* __restrict__ a, uint32_t m, const float* __restrict__ b, uint32_t n,
+                float* __restrict__ out, uint32_t* __restrict__ error_flag) {
+    using L = JoinLayout<D>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* A = reinterpret_cast<float*>(smem);
+    float* B = reinterpret_cast<float*>(smem + L::tile_bytes);
+    uint32_t* ids = reinterpret_cast<uint32_t*>(smem + 2 * L::tile_bytes);
+    float* zero = reinterpret_cast<float*>(ids + kTile);
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+    if (tid < kTile) ids[tid] = tid;
+    for (int j = tid; j < D; j += kJoinThreads) zero[j] = 0.0f;
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
+    if (tid == 0) {
+        tc::mbar_init(&mbar, 1);
+        tc::fence_barrier_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    stage_centred<D>(A, ids, m, a, D, zero);
+    stage_centred<D>(B, ids, n, b, D, zero);
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        tc::fence_after_sync();
+        tc::issue_tile_tf32(tmem, tc::smem_u32(A), tc::smem_u32(B), kTile, kTile, L::KP, tc::idesc_tf32(kTile, kTile));
+        tc::mma_commit(&mbar);
+    }
+    const bool done = tc::mbar_wait(&mbar, 0);
+    if (__syncthreads_or(!done)) {
+        if (tid == 0) atomicExch(error_flag, 1u);
+    } else {
+        tc::fence_after_sync();
+        const int quarter = warp % 4, half = warp / 4, row = quarter * kWarp + lane;
+        for (int cc = 0; cc < 4; ++cc) {
+            const int j0 = half * 64 + cc * 16;
+            float g[16];
+            tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+                if (static_cast<uint32_t>(row) < m && static_cast<uint32_t>(j0 + u) < n)
+                    out[static_cast<size_t>(row) * n + j0 + u] = g[u];
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, kTile);
+    }
+}
+
+void device_scan(Context& c, const uint32_t* in, uint64_t n, unsigned long long* out) {
+    const uint32_t tiles = static_cast<uint32_t>((n + kScanTile - 1) / kScanTile);
+    auto* tsum = static_cast<unsigned long long*>(scratch(c, "scan_tiles", (tiles + 1) * sizeof(unsigned long long)));
+    k_scan_reduce<<<tiles, kScanThreads, 0, c.stream>>>(in, n, tsum);
+    k_scan_tiles<<<1, kScanThreads, 0, c.stream>>>(tsum, tiles);
+    k_scan_apply<<<tiles, kScanThreads, 0, c.stream>>>(in, n, tsum, out);
+    c.launches += 3;
+    KNNG_CUDA(cudaGetLastError());
+}
+
+// Survivor records (8 bytes each) held at once by one store round.
+constexpr uint64_t kMaxRoundRecords = 1ull << 31;
+
 }  // namespace
 
-uint64_t run_refine(Context& c) {
-    if (c.n == 0) return 0;
-    const int K = static_cast<int>(c.k);
-    uint32_t* snap = static_cast<uint32_t*>(scratch(c, "refine_snap", static_cast<size_t>(c.n) * K * sizeof(uint32_t)));
-    const uint32_t sblocks = std::min<uint32_t>((c.n + kRefWarps - 1) / kRefWarps, 148 * 8);
-    k_snapshot<<<sblocks, kRefWarps * kWarp, 0, c.stream>>>(c.set_id, c.n, K, snap);
+void run_tile_gram(Context& c, uint32_t d, const float* d_a, uint32_t m, const float* d_b, uint32_t n, float* d_out) {
+    auto* err = static_cast<uint32_t*>(scratch(c, "gram_error", sizeof(uint32_t)));
+    KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
+    KNNG_DISPATCH_D(d, {
+        const size_t smem = 2 * JoinLayout<D>::tile_bytes + kTile * 4 + D * 4;
+        auto kern = k_tile_gram<D>;
+        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        kern<<<1, kJoinThreads, smem, c.stream>>>(d_a, m, d_b, n, d_out, err);
+    });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
+    uint32_t h = 0;
+    download(c, &h, err, 1);
+    if (h) fail(KNNG_ERR_CUDA, "tensor-core tile: the MMA completion wait timed out");
+}
+
+uint64_t run_refine_pointwise(Context& c, const uint32_t* snap, const uint32_t* d_list, uint32_t count) {
+    const int K = static_cast<int>(c.k);
     const uint32_t cap = pow2_at_least(static_cast<uint32_t>(K * K));
-    const uint32_t blocks = std::min<uint32_t>((c.n + kRefWarps - 1) / kRefWarps, 148 * 2);
+    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((count + kRefWarps - 1) / kRefWarps, 148 * 5));
     auto* keys = static_cast<unsigned long long*>(
         scratch(c, "refine_keys", static_cast<size_t>(blocks) * kRefWarps * cap * sizeof(unsigned long long)));
     auto* changed = static_cast<uint32_t*>(scratch(c, "refine_changed", sizeof(uint32_t)));
     KNNG_CUDA(cudaMemsetAsync(changed, 0, sizeof(uint32_t), c.stream));
     KNNG_DISPATCH_D(c.d, {
         k_refine<D><<<blocks, kRefWarps * kWarp, 0, c.stream>>>(snap, c.points, c.ld, c.set_dist, c.set_id,
-                                                               c.set_size, c.set_maxslot, c.set_bound, K, c.n, keys,
-                                                               cap, changed);
+                                                               c.set_size, c.set_maxslot, c.set_bound, K, count,
+                                                               d_list, keys, cap, changed);
     });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     uint32_t h = 0;
     download(c, &h, changed, 1);
     return h;
+}
+
+uint64_t run_refine(Context& c) {
+    if (c.n == 0) return 0;
+    const int K = static_cast<int>(c.k);
+    const uint32_t n = c.n;
+    uint32_t* snap = static_cast<uint32_t*>(scratch(c, "refine_snap", static_cast<size_t>(n) * K * sizeof(uint32_t)));
+    const uint32_t sblocks = std::min<uint32_t>((n + kSnapWarps - 1) / kSnapWarps, 148 * 8);
+    k_snapshot<<<sblocks, kSnapWarps * kWarp, 0, c.stream>>>(c.set_id, n, K, snap);
+    ++c.launches;
+    KNNG_CUDA(cudaGetLastError());
+    if (c.refine_mode == 1) return run_refine_pointwise(c, snap, nullptr, n);
+
+    Context::RefineRecord rec;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) KNNG_CUDA(cudaEventCreate(&e));
+    KNNG_CUDA(cudaEventRecord(ev[0], c.stream));
+    // Reverse lists.
+    auto* cnt = static_cast<uint32_t*>(scratch(c, "rev_count", (static_cast<size_t>(n) + 1) * sizeof(uint32_t)));
+    auto* cur = static_cast<uint32_t*>(scratch(c, "rev_cursor", (static_cast<size_t>(n) + 1) * sizeof(uint32_t)));
+    auto* off = static_cast<unsigned long long*>(
+        scratch(c, "rev_offsets", (static_cast<size_t>(n) + 1) * sizeof(unsigned long long)));
+    auto* rev = static_cast<uint32_t*>(scratch(c, "rev_ids", static_cast<size_t>(n) * K * sizeof(uint32_t)));
+    KNNG_CUDA(cudaMemsetAsync(cnt, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(cur, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
+    const uint32_t wblocks = std::min<uint32_t>((n + 7) / 8, 148 * 16);
+    k_rev_count<<<wblocks, 256, 0, c.stream>>>(snap, n, K, cnt);
+    device_scan(c, cnt, n, off);
+    k_rev_fill<<<wblocks, 256, 0, c.stream>>>(snap, n, K, off, cur, rev);
+    c.launches += 2;
+    KNNG_CUDA(cudaGetLastError());
+
+    // Join, counting pass: survivors per point.
+    auto* scount = static_cast<uint32_t*>(scratch(c, "surv_count", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* sfill = static_cast<uint32_t*>(scratch(c, "surv_fill", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* soff = static_cast<unsigned long long*>(
+        scratch(c, "surv_offsets", (static_cast<size_t>(n) + 1) * sizeof(unsigned long long)));
+    auto* err = static_cast<uint32_t*>(scratch(c, "join_error", sizeof(uint32_t)));
+    auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 8 * sizeof(unsigned long long)));
+    KNNG_CUDA(cudaMemsetAsync(scount, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(jc, 0, 8 * sizeof(unsigned long long), c.stream));
+    auto join = [&](int mode, uint32_t lo, uint32_t hi, unsigned long long base, unsigned long long* out) {
+        KNNG_DISPATCH_D(c.d, {
+            const size_t smem = JoinLayout<D>::bytes;
+            auto kern = k_join<D>;
+            KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+            kern<<<148, kJoinThreads, smem, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K, n,
+                                                        mode, lo, hi, scount, soff, base, sfill, out, err,
+                                                        mode == 0 ? jc : jc + 5);
+        });
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
+    };
+    join(0, 0, n, 0, nullptr);
+    device_scan(c, scount, n, soff);
+    // Store rounds over point ranges whose records fit kMaxRoundRecords.
+    std::vector<unsigned long long> hoff(static_cast<size_t>(n) + 1);
+    download(c, hoff.data(), soff, hoff.size());
+    uint32_t herr = 0;
+    download(c, &herr, err, 1);
+    if (herr) {
+        for (auto& e : ev) cudaEventDestroy(e);
+        fail(KNNG_ERR_CUDA, "tensor-core join: an MMA completion wait timed out");
+    }
+    const unsigned long long total = hoff[n];
+    unsigned long long round_cap = std::min<unsigned long long>(total, kMaxRoundRecords);
+    auto* surv = static_cast<unsigned long long*>(scratch(c, "surv_keys", (round_cap + 1) * sizeof(unsigned long long)));
+    uint32_t max_count = 0;
+    for (uint32_t i = 0; i < n; ++i) max_count = std::max<uint32_t>(max_count, static_cast<uint32_t>(hoff[i + 1] - hoff[i]));
+    auto* big = static_cast<uint32_t*>(scratch(c, "apply_big", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* counters = static_cast<uint32_t*>(scratch(c, "apply_counters", 2 * sizeof(uint32_t)));
+    KNNG_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(uint32_t), c.stream));
+    const uint32_t big_cap = pow2_at_least(std::max<uint32_t>(max_count, 2));
+    const uint32_t big_blocks = 148 * 2;
+    unsigned long long* big_keys = nullptr;
+    if (max_count > static_cast<uint32_t>(kApplyCap))
+        big_keys = static_cast<unsigned long long*>(
+            scratch(c, "apply_big_keys", static_cast<size_t>(big_blocks) * kRefWarps * big_cap * sizeof(unsigned long long)));
+    float ms_join = 0, ms_apply = 0;
+    KNNG_CUDA(cudaEventRecord(ev[1], c.stream));
+    uint32_t lo = 0;
+    while (lo < n) {
+        uint32_t hi = lo + 1;
+        // Largest hi with hoff[hi] - hoff[lo] <= round_cap (at least one point).
+        uint32_t a = lo + 1, b = n;
+        while (a < b) {
+            const uint32_t mid = a + (b - a + 1) / 2;
+            if (hoff[mid] - hoff[lo] <= round_cap) a = mid; else b = mid - 1;
+        }
+        hi = std::max(a, lo + 1);
+        const unsigned long long base = hoff[lo];
+        if (hoff[hi] - base > round_cap) fail(KNNG_ERR_BUDGET, "one point's survivors exceed the round capacity");
+        cudaEvent_t r0, r1, r2;
+        KNNG_CUDA(cudaEventCreate(&r0));
+        KNNG_CUDA(cudaEventCreate(&r1));
+        KNNG_CUDA(cudaEventCreate(&r2));
+        KNNG_CUDA(cudaEventRecord(r0, c.stream));
+        if (hoff[hi] > base) {
+            KNNG_CUDA(cudaMemsetAsync(sfill + lo, 0, static_cast<size_t>(hi - lo) * sizeof(uint32_t), c.stream));
+            join(1, lo, hi, base, surv);
+        }
+        KNNG_CUDA(cudaEventRecord(r1, c.stream));
+        KNNG_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t), c.stream));
+        const uint32_t ablocks = std::min<uint32_t>((hi - lo + kRefWarps - 1) / kRefWarps, 148 * 16);
+        k_apply<<<ablocks, kRefWarps * kWarp, 0, c.stream>>>(lo, hi, K, scount, soff, base, surv, c.set_dist,
+                                                             c.set_id, c.set_size, c.set_maxslot, c.set_bound, big,
+                                                             counters, counters + 1);
+        ++c.launches;
+        if (big_keys) {
+            k_apply_big<<<big_blocks, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, soff, base, surv,
+                                                                       big_keys, big_cap, c.set_dist, c.set_id,
+                                                                       c.set_size, c.set_maxslot, c.set_bound,
+                                                                       counters + 1);
+            ++c.launches;
+        }
+        KNNG_CUDA(cudaGetLastError());
+        KNNG_CUDA(cudaEventRecord(r2, c.stream));
+        KNNG_CUDA(cudaEventSynchronize(r2));
+        float a_ms = 0, b_ms = 0;
+        KNNG_CUDA(cudaEventElapsedTime(&a_ms, r0, r1));
+        KNNG_CUDA(cudaEventElapsedTime(&b_ms, r1, r2));
+        ms_join += a_ms;
+        ms_apply += b_ms;
+        cudaEventDestroy(r0);
+        cudaEventDestroy(r1);
+        cudaEventDestroy(r2);
+        ++rec.overflow;  // rounds
+        lo = hi;
+    }
+    KNNG_CUDA(cudaEventRecord(ev[2], c.stream));
+    uint32_t h[2] = {0, 0};
+    unsigned long long hc[8] = {0};
+    download(c, h, counters, 2);
+    download(c, hc, jc, 8);
+    download(c, &herr, err, 1);
+    if (herr) {
+        for (auto& e : ev) cudaEventDestroy(e);
+        fail(KNNG_ERR_CUDA, herr == 2 ? "tensor-core join: store pass disagreed with the counting pass"
+                                      : "tensor-core join: an MMA completion wait timed out");
+    }
+    uint64_t changed = h[1];
+    KNNG_CUDA(cudaEventRecord(ev[3], c.stream));
+    KNNG_CUDA(cudaEventSynchronize(ev[3]));
+    float ms_count = 0;
+    KNNG_CUDA(cudaEventElapsedTime(&ms_count, ev[0], ev[1]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    rec.ms_join = ms_count + ms_join;
+    rec.ms_apply = ms_apply;
+    rec.ms_fallback = 0;
+    rec.pairs = hc[0];
+    rec.filter_pass = hc[1];
+    rec.member_skip = hc[2];
+    rec.exact = hc[3];
+    rec.emits = hc[4];
+    c.last_refine = rec;
+    return changed;
 }
 
 }  // namespace knng

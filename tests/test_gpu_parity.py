@@ -206,6 +206,45 @@ def test_edge_cases(oracle_lib, ctx):
     assert_sets_equal(ctx.sets(), o.sets(), "tiny buckets")
 
 
+@pytest.mark.parametrize("d,m,n", [(100, 128, 128), (100, 77, 113), (64, 128, 16), (128, 5, 128)])
+def test_tensor_core_tile_against_fp64(ctx, d, m, n):
+    """One tcgen05 kind::tf32 tile against an FP64 matmul: the error stays
+    inside the TF32 operand-rounding bound the refinement filter relies on."""
+    from sigmod23ann_b200.api import debug_tile_gram
+
+    rng = np.random.default_rng(d + m + n)
+    a = rng.standard_normal((m, d)).astype(np.float32)
+    b = rng.standard_normal((n, d)).astype(np.float32)
+    g = debug_tile_gram(ctx, a, b)
+    ref = a.astype(np.float64) @ b.astype(np.float64).T
+    scale = np.abs(a).astype(np.float64) @ np.abs(b).astype(np.float64).T
+    err = np.abs(g - ref)
+    assert (err <= 2.0 ** -8 * scale + 1e-6).all(), float((err / scale).max())
+    # and it is a TF32 product, not something coarser
+    assert float((err / scale).max()) < 2.0 ** -9
+
+
+def test_refine_join_equals_pointwise(knng_lib, monkeypatch):
+    """The tensor-core local join and the one-warp-per-point pass leave
+    identical sets."""
+    pts = workloads.gaussian_mixture(n=20_000, d=100, clusters=32, sigma=0.15, seed=3)
+    p = default_params(reps=2, max_leaf=257, max_leaf_odd=0, lloyd_iters=2, refine=0, seed=9)
+    with KnngContext(0) as a:
+        a.build(pts, p)
+        s0 = a.sets()
+        ch_a = a.refine()
+        sa = a.sets()
+    monkeypatch.setenv("KNNG_REFINE", "pointwise")
+    with KnngContext(0) as b:
+        b.load_points(pts)
+        b.reset_sets(100)
+        b.set_sets(s0)
+        ch_b = b.refine()
+        sb = b.sets()
+    assert ch_a == ch_b
+    assert_sets_equal(sa, sb, "join vs pointwise")
+
+
 def test_invalid_arguments(ctx):
     with pytest.raises(KnngError) as e:
         ctx.build(np.zeros((10, 99), np.float32))
