@@ -136,6 +136,45 @@ __device__ __forceinline__ float canonical_distance4(const float4* __restrict__ 
     return acc;
 }
 
+// The same order as canonical_distance4, one 8-dimension step at a time
+// (four float4 loads live per step): for callers with little register room.
+template <int D>
+__device__ __forceinline__ float canonical_distance4_lean(const float4* __restrict__ a, const float4* __restrict__ b) {
+    static_assert(D % 4 == 0, "float4 path needs D % 4 == 0");
+    constexpr int M = D / 8 * 8;
+    float lane[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
+#pragma unroll 1
+    for (int q = 0; q < M / 4; q += 2) {
+        const float4 x0 = a[q], x1 = a[q + 1];
+        const float4 y0 = b[q], y1 = b[q + 1];
+        float d;
+        d = __fsub_rn(x0.x, y0.x); lane[0] = __fmaf_rn(d, d, lane[0]);
+        d = __fsub_rn(x0.y, y0.y); lane[1] = __fmaf_rn(d, d, lane[1]);
+        d = __fsub_rn(x0.z, y0.z); lane[2] = __fmaf_rn(d, d, lane[2]);
+        d = __fsub_rn(x0.w, y0.w); lane[3] = __fmaf_rn(d, d, lane[3]);
+        d = __fsub_rn(x1.x, y1.x); lane[4] = __fmaf_rn(d, d, lane[4]);
+        d = __fsub_rn(x1.y, y1.y); lane[5] = __fmaf_rn(d, d, lane[5]);
+        d = __fsub_rn(x1.z, y1.z); lane[6] = __fmaf_rn(d, d, lane[6]);
+        d = __fsub_rn(x1.w, y1.w); lane[7] = __fmaf_rn(d, d, lane[7]);
+    }
+    float acc = 0.0f;
+#pragma unroll
+    for (int l = 0; l < 8; ++l) acc = __fadd_rn(acc, lane[l]);
+#pragma unroll
+    for (int q = M / 4; q < D / 4; ++q) {
+        const float4 x = a[q];
+        const float4 y = b[q];
+        float d0 = __fsub_rn(x.x, y.x), d1 = __fsub_rn(x.y, y.y), d2 = __fsub_rn(x.z, y.z), d3 = __fsub_rn(x.w, y.w);
+        acc = __fadd_rn(acc, __fmul_rn(d0, d0));
+        acc = __fadd_rn(acc, __fmul_rn(d1, d1));
+        acc = __fadd_rn(acc, __fmul_rn(d2, d2));
+        acc = __fadd_rn(acc, __fmul_rn(d3, d3));
+    }
+    return acc;
+}
+
 // ---------------------------------------------------------- neighbour sets
 //
 // Tie order of getMaxIdx: among slots holding the maximum distance, the one

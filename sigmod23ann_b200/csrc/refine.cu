@@ -290,26 +290,58 @@ struct JoinLayout {
     static constexpr int KP = (D + 7) / 8 * 8;  // K padded to the MMA step (8 tf32)
     static constexpr int CH = KP / 4;           // 16-byte chunks per row
     static constexpr size_t tile_bytes = static_cast<size_t>(kTile) * KP * 4;
-    // A', B' (centred TF32 tiles), original B rows, member masks, per-row scalars.
-    static constexpr size_t orig_bytes = static_cast<size_t>(kTile) * D * 4;
-    static constexpr size_t bytes = 2 * tile_bytes + orig_bytes + kTile * 4 * 4 + 5 * kTile * 4 + 128 * 4;
+    // A', B' (centred TF32 tiles) and per-row scalars (about 108 KB at D = 100:
+    // two CTAs per SM).  Once the MMA has consumed A' and B', their space holds
+    // p's sorted lists, then the original FP32 rows.
+    static_assert(tile_bytes >= static_cast<size_t>(kTile) * D * 4, "original rows must fit in a tile");
+    static_assert(2 * tile_bytes >= static_cast<size_t>(kTile) * kMaxK * 4, "lists must fit in the two tiles");
+    static constexpr size_t bytes = 2 * tile_bytes + 5 * kTile * 4 + 128 * 4 + 16;
 };
 
-// rows[r] (r < count, else zeros) minus `centre`, into a chunk-major tile.
+// rows[r] (r < count and ids[r] != kNone, else zeros) minus `centre`, into a
+// chunk-major tile.  Lane l of a warp handles row (8g + l % 8), chunk
+// (4h + l / 8): every global sector read is used whole and each quarter-warp's
+// 16-byte shared stores land on distinct banks.
 template <int D>
 __device__ __forceinline__ void stage_centred(float* __restrict__ tile, const uint32_t* __restrict__ ids,
                                               uint32_t count, const float* __restrict__ pts, int ld,
                                               const float* __restrict__ centre) {
     constexpr int CH = JoinLayout<D>::CH;
-    for (int f = threadIdx.x; f < kTile * CH; f += kJoinThreads) {
-        const int r = f % kTile, ch = f / kTile;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
-            const float4 x = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + ch);
-            const float4 m = reinterpret_cast<const float4*>(centre)[ch];
-            v = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z), __fsub_rn(x.w, m.w));
+    constexpr int CG = (CH + 3) / 4;                                   // chunk groups
+    constexpr int ITER = ((kTile / 8) * CG + kJoinThreads / kWarp - 1) / (kJoinThreads / kWarp);
+    constexpr int BATCH = 4;
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    const int rl = lane & 7, cl = lane >> 3;
+#pragma unroll 1
+    for (int b0 = 0; b0 < ITER; b0 += BATCH) {
+    float4 v[BATCH];
+    // A batch of loads is issued before its stores.
+#pragma unroll
+    for (int bi = 0; bi < BATCH; ++bi) {
+        const int it = b0 + bi;
+        const int w = warp + it * (kJoinThreads / kWarp);
+        const int r = (w % (kTile / 8)) * 8 + rl;
+        const int ch = (w / (kTile / 8)) * 4 + cl;
+        v[bi] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (it < ITER && w < (kTile / 8) * CG && ch < CH && static_cast<uint32_t>(r) < count && 4 * ch < D &&
+            ids[r] != kNone)
+            v[bi] = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + ch);
+    }
+#pragma unroll
+    for (int bi = 0; bi < BATCH; ++bi) {
+        const int it = b0 + bi;
+        const int w = warp + it * (kJoinThreads / kWarp);
+        const int r = (w % (kTile / 8)) * 8 + rl;
+        const int ch = (w / (kTile / 8)) * 4 + cl;
+        if (it < ITER && w < (kTile / 8) * CG && ch < CH) {
+            float4 x = v[bi];
+            if (static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
+                const float4 m = reinterpret_cast<const float4*>(centre)[ch];
+                x = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z), __fsub_rn(x.w, m.w));
+            }
+            *reinterpret_cast<float4*>(reinterpret_cast<unsigned char*>(tile) + tc::chunk_offset(r, 4 * ch, kTile)) = x;
         }
-        *reinterpret_cast<float4*>(reinterpret_cast<unsigned char*>(tile) + tc::chunk_offset(r, 4 * ch, kTile)) = v;
+    }
     }
 }
 
@@ -327,22 +359,37 @@ __device__ __forceinline__ float tile_norm(const float* __restrict__ tile, int r
     return s;
 }
 
-// Copies rows ids[r] (r < count) into a row-major tile of D floats per row.
+// Copies rows ids[r] (r < count, ids[r] != kNone) into a row-major tile of D
+// floats per row; every load of a thread is issued before its stores.
 template <int D>
 __device__ __forceinline__ void stage_rows(float* __restrict__ dst, const uint32_t* __restrict__ ids, uint32_t count,
                                            const float* __restrict__ pts, int ld) {
     constexpr int Q = D / 4;
-    for (uint32_t f = threadIdx.x; f < count * Q; f += kJoinThreads) {
-        const uint32_t r = f / Q, q = f % Q;
-        reinterpret_cast<float4*>(dst)[f] =
-            __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + q);
+    constexpr int BATCH = 4;
+    const uint32_t total = count * Q;
+#pragma unroll 1
+    for (uint32_t f0 = threadIdx.x; f0 < total; f0 += BATCH * kJoinThreads) {
+        float4 v[BATCH];
+#pragma unroll
+        for (int bi = 0; bi < BATCH; ++bi) {
+            const uint32_t f = f0 + bi * kJoinThreads;
+            const uint32_t r = f / Q, q = f % Q;
+            if (f < total && ids[r] != kNone)
+                v[bi] = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + q);
+        }
+#pragma unroll
+        for (int bi = 0; bi < BATCH; ++bi) {
+            const uint32_t f = f0 + bi * kJoinThreads;
+            if (f < total && ids[f / Q] != kNone) reinterpret_cast<float4*>(dst)[f] = v[bi];
+        }
     }
 }
+
 
 // mode 0 counts survivors per point into surv_count; mode 1 writes them at
 // surv[surv_off[p] - base + cursor] for points p in [p_lo, p_hi).
 template <int D>
-__global__ void __launch_bounds__(kJoinThreads, 1)
+__global__ void __launch_bounds__(kJoinThreads, 2)
     k_join(const uint32_t* __restrict__ snap, const unsigned long long* __restrict__ rev_off,
            const uint32_t* __restrict__ rev, const float* __restrict__ pts, int ld, const float* __restrict__ bound,
            const uint32_t* __restrict__ set_size, int K, uint32_t n, int mode, uint32_t p_lo, uint32_t p_hi,
@@ -353,9 +400,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     extern __shared__ __align__(1024) unsigned char smem[];
     float* A = reinterpret_cast<float*>(smem);
     float* B = reinterpret_cast<float*>(smem + L::tile_bytes);
-    float* Borig = reinterpret_cast<float*>(smem + 2 * L::tile_bytes);
-    uint32_t* masks = reinterpret_cast<uint32_t*>(smem + 2 * L::tile_bytes + L::orig_bytes);
-    float* normA = reinterpret_cast<float*>(masks + kTile * 4);
+    float* normA = reinterpret_cast<float*>(smem + 2 * L::tile_bytes);
     float* normB = normA + kTile;
     float* bnd = normB + kTile;
     uint32_t* pid = reinterpret_cast<uint32_t*>(bnd + kTile);
@@ -364,6 +409,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     __shared__ uint32_t ncols_s;
+    __shared__ uint32_t fullrow[kTile];
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
     if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
     if (tid == 0) {
@@ -380,19 +426,30 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     unsigned long long n_pairs = 0, n_pass = 0, n_member = 0, n_exact = 0, n_emit = 0;
     const int quarter = warp % 4, half = warp / 4;
     const int row = quarter * kWarp + lane;  // TMEM lane / tile row of this thread
+    const unsigned lt = (1u << lane) - 1u;
     for (uint32_t q = blockIdx.x; q < n && healthy; q += gridDim.x) {
         const unsigned long long rb = rev_off[q], re = rev_off[q + 1];
         if (rb == re) continue;
         // Columns: the distinct ids of S(q), ascending.
         if (warp == 0) {
             const uint32_t* sq = snap + static_cast<size_t>(q) * K;
+            uint32_t v[kSlotsPerLane];
+#pragma unroll
+            for (int i = 0; i < kSlotsPerLane; ++i) {
+                const int a = i * kWarp + lane;
+                v[i] = a < K ? __ldg(sq + a) : kNone;
+            }
             uint32_t base = 0;
-            for (int a0 = 0; a0 < K; a0 += kWarp) {
-                const int a = a0 + lane;
-                const uint32_t v = a < K ? sq[a] : kNone;
-                const bool keep = a < K && (a == 0 || sq[a - 1] != v);
+#pragma unroll
+            for (int i = 0; i < kSlotsPerLane; ++i) {
+                const int a = i * kWarp + lane;
+                // Previous entry: from the lane below, or lane 31 of the last step.
+                uint32_t prev = __shfl_up_sync(kFull, v[i], 1);
+                const uint32_t wrap = i > 0 ? __shfl_sync(kFull, v[i > 0 ? i - 1 : 0], kWarp - 1) : kNone;
+                if (lane == 0) prev = wrap;
+                const bool keep = a < K && (a == 0 || prev != v[i]);
                 const unsigned m = __ballot_sync(kFull, keep);
-                if (keep) cid[base + __popc(m & ((1u << lane) - 1u))] = v;
+                if (keep) cid[base + __popc(m & lt)] = v[i];
                 base += __popc(m);
             }
             if (lane == 0) ncols_s = base;
@@ -401,7 +458,6 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
         __syncthreads();
         const uint32_t nc = ncols_s;
         stage_centred<D>(B, cid, nc, pts, ld, centre);
-        stage_rows<D>(Borig, cid, nc, pts, ld);
         __syncthreads();
         if (tid < kTile) normB[tid] = tile_norm<D>(B, tid);
         for (unsigned long long cb = rb; cb < re && healthy; cb += kTile) {
@@ -412,25 +468,12 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                 if (p != kNone && (p < p_lo || p >= p_hi)) p = kNone;
                 pid[tid] = p;
                 bnd[tid] = p != kNone ? bound[p] : 0.0f;
+                // A set that is not full lists its empty slots as id 0.
+                fullrow[tid] = p != kNone && set_size[p] == static_cast<uint32_t>(K) ? 1u : 0u;
                 any = p != kNone;
             }
-            for (int t = tid; t < kTile * 4; t += kJoinThreads) masks[t] = 0u;
             if (!__syncthreads_or(any)) continue;
             stage_centred<D>(A, pid, m, pts, ld, centre);
-            // Member masks: bit j of row r set when column j is in S(pid[r]).
-            for (uint32_t f = tid; f < m * static_cast<uint32_t>(K); f += kJoinThreads) {
-                const uint32_t r = f / K, a = f % K;
-                const uint32_t p = pid[r];
-                if (p == kNone) continue;
-                const uint32_t v = snap[static_cast<size_t>(p) * K + a];
-                if (v == 0 && set_size[p] < static_cast<uint32_t>(K)) continue;  // empty slots read as id 0
-                int lo = 0, hi = static_cast<int>(nc);
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (cid[mid] < v) lo = mid + 1; else hi = mid;
-                }
-                if (lo < static_cast<int>(nc) && cid[lo] == v) atomicOr(&masks[r * 4 + (lo >> 5)], 1u << (lo & 31));
-            }
             __syncthreads();
             if (tid < kTile) normA[tid] = tile_norm<D>(A, tid);
             tc::fence_proxy_async();
@@ -449,52 +492,160 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                 break;
             }
             tc::fence_after_sync();
+            // p's list S(p), sorted, staged into the space A' and B' occupied with
+            // an odd row stride (conflict-free binary searches by row).
+            const int KS = static_cast<size_t>(kTile) * (K | 1) * 4 <= 2 * L::tile_bytes ? (K | 1) : K;
+            const uint32_t* lists = reinterpret_cast<const uint32_t*>(A);
+            {
+                uint32_t* dst = reinterpret_cast<uint32_t*>(A);
+                const uint32_t total = m * static_cast<uint32_t>(K);
+                if ((K & 3) == 0) {
+                    // 16-byte loads, a batch of eight in flight per thread.
+                    const uint32_t KV = static_cast<uint32_t>(K) / 4, tv = total / 4;
+#pragma unroll 1
+                    for (uint32_t f0 = tid; f0 < tv; f0 += 8 * kJoinThreads) {
+                        uint4 v[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            const uint32_t f = f0 + u * kJoinThreads;
+                            v[u] = make_uint4(kNone, kNone, kNone, kNone);
+                            if (f < tv) {
+                                const uint32_t r = f / KV, a = f - r * KV;
+                                const uint32_t pr = pid[r];
+                                if (pr != kNone)
+                                    v[u] = __ldg(reinterpret_cast<const uint4*>(snap + static_cast<size_t>(pr) * K) + a);
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            const uint32_t f = f0 + u * kJoinThreads;
+                            if (f < tv) {
+                                const uint32_t r = f / KV, a = 4 * (f - r * KV);
+                                uint32_t* d = dst + r * KS + a;
+                                d[0] = v[u].x;
+                                d[1] = v[u].y;
+                                d[2] = v[u].z;
+                                d[3] = v[u].w;
+                            }
+                        }
+                    }
+                } else {
+#pragma unroll 1
+                    for (uint32_t f0 = tid; f0 < total; f0 += 4 * kJoinThreads) {
+                        uint32_t v[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const uint32_t f = f0 + u * kJoinThreads;
+                            v[u] = kNone;
+                            if (f < total) {
+                                const uint32_t r = f / K, a = f - r * K;
+                                const uint32_t pr = pid[r];
+                                if (pr != kNone) v[u] = __ldg(snap + static_cast<size_t>(pr) * K + a);
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const uint32_t f = f0 + u * kJoinThreads;
+                            if (f < total) {
+                                const uint32_t r = f / K, a = f - r * K;
+                                dst[r * KS + a] = v[u];
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            // Filter: bit (cc*16 + u) of `todo` marks column half*64 + cc*16 + u
+            // as a pair that may beat bound(p) and is not a member of S(p).
             const uint32_t p = row < static_cast<int>(m) ? pid[row] : kNone;
             const float bp = row < static_cast<int>(m) ? bnd[row] : 0.0f;
-            const float na = normA[row];
-            const float4* prow = reinterpret_cast<const float4*>(pts + static_cast<size_t>(p == kNone ? 0 : p) * ld);
+            unsigned long long todo = 0;
+            {
+                const float na = normA[row];
 #pragma unroll 1
-            for (int cc = 0; cc < 4; ++cc) {
-                const int j0 = half * 64 + cc * 16;
-                float g[16];
-                tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
-                tc::tmem_wait_ld();
-                if (p == kNone) continue;
-                // Tensor-core filter: bit u set when the pair may beat bound(p).
-                // |approx - exact| <= 2^-7 (|x'|^2 + |y'|^2) + 2^-16 |approx| covers the TF32
-                // operands, FP32 accumulation, centring and the reference's summation order.
-                uint32_t pass = 0;
+                for (int cc = 0; cc < 4; ++cc) {
+                    const int j0 = half * 64 + cc * 16;
+                    float g[16];
+                    tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
+                    tc::tmem_wait_ld();
+                    // |approx - exact| <= 2^-7 (|x'|^2 + |y'|^2) + 2^-16 |approx| covers the TF32
+                    // operands, FP32 accumulation, centring and the reference's summation order.
+                    uint32_t pass = 0;
+                    float nbv[16];
 #pragma unroll
-                for (int u = 0; u < 16; ++u) {
-                    const float nb = normB[j0 + u];
-                    const float approx = na + nb - 2.0f * g[u];
-                    const float margin = 0.0078125f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + 1e-30f;
-                    if (j0 + u < static_cast<int>(nc) && approx - margin < bp) pass |= 1u << u;
+                    for (int u4 = 0; u4 < 4; ++u4) {
+                        const float4 t4 = reinterpret_cast<const float4*>(normB + j0)[u4];
+                        nbv[4 * u4 + 0] = t4.x;
+                        nbv[4 * u4 + 1] = t4.y;
+                        nbv[4 * u4 + 2] = t4.z;
+                        nbv[4 * u4 + 3] = t4.w;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const float nb = nbv[u];
+                        const float approx = na + nb - 2.0f * g[u];
+                        const float margin = 0.0078125f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + 1e-30f;
+                        if (approx - margin < bp) pass |= 1u << u;
+                    }
+                    const int valid_cols = max(0, min(16, static_cast<int>(nc) - j0));
+                    pass &= valid_cols == 16 ? 0xFFFFu : ((1u << valid_cols) - 1u);
+                    if (p == kNone) pass = 0;
+                    // Members of S(p) are rejected by the set update: drop them.
+                    // (A set that is not full lists its empty slots as id 0.)
+                    uint32_t keep = pass;
+                    const uint32_t* mylist = lists + row * KS;
+                    const bool full = row < static_cast<int>(m) && fullrow[row] != 0u;
+                    uint32_t scan = pass;
+                    while (scan) {
+                        const int u = __ffs(scan) - 1;
+                        scan &= scan - 1;
+                        const uint32_t c = cid[j0 + u];
+                        if (c == 0 && !full) continue;
+                        int lo = 0, hi = K;
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (mylist[mid] < c) lo = mid + 1; else hi = mid;
+                        }
+                        if (lo < K && mylist[lo] == c) keep &= ~(1u << u);
+                    }
+                    if (p != kNone) {
+                        n_pairs += valid_cols;
+                        n_pass += __popc(pass);
+                        n_member += __popc(pass & ~keep);
+                    }
+                    todo |= static_cast<unsigned long long>(keep) << (cc * 16);
                 }
-                n_pairs += static_cast<unsigned long long>(max(0, min(16, static_cast<int>(nc) - j0)));
-                n_pass += __popc(pass);
-                const uint32_t members = (masks[row * 4 + (j0 >> 5)] >> (j0 & 31)) & 0xFFFFu;
-                n_member += __popc(pass & members);
-                uint32_t todo = pass & ~members;
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+            // The tiles are consumed: refill their space with the original FP32
+            // rows (row-major, D floats) for the exact distances.
+            float* Aorig = A;
+            float* Bo = B;
+            stage_rows<D>(Aorig, pid, m, pts, ld);
+            stage_rows<D>(Bo, cid, nc, pts, ld);
+            __syncthreads();
+            if (p != kNone) {
+                const float4* prow = reinterpret_cast<const float4*>(Aorig + row * D);
 #pragma unroll 1
                 while (todo) {
-                    const int u = __ffs(todo) - 1;
+                    const int b = __ffsll(todo) - 1;
                     todo &= todo - 1;
-                    const int j = j0 + u;
+                    const int j = half * 64 + b;
                     const uint32_t c = cid[j];
                     if (c == p) continue;
                     ++n_exact;
-                    const float d = canonical_distance4<D>(reinterpret_cast<const float4*>(Borig + j * D), prow);
+                    const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(Bo + j * D), prow);
                     if (d < bp) {
                         ++n_emit;
                         if (mode == 0) {
                             atomicAdd(&surv_count[p], 1u);
                         } else {
-                            const uint32_t slot = atomicAdd(&surv_fill[p], 1u);
+                            const uint32_t s2 = atomicAdd(&surv_fill[p], 1u);
                             // The store pass repeats the counting pass exactly; the
                             // guard keeps a disagreement from writing past p's range.
-                            if (slot < surv_count[p])
-                                surv[surv_off[p] - surv_base + slot] =
+                            if (s2 < surv_count[p])
+                                surv[surv_off[p] - surv_base + s2] =
                                     (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
                             else
                                 atomicExch(error_flag, 2u);
@@ -502,8 +653,12 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                     }
                 }
             }
-            tc::fence_before_sync();
             __syncthreads();
+            // The next chunk restages B' (its space now holds original rows).
+            if (cb + kTile < re) {
+                stage_centred<D>(B, cid, nc, pts, ld, centre);
+                __syncthreads();
+            }
         }
     }
     atomicAdd(&counters[0], n_pairs);
@@ -749,10 +904,10 @@ uint64_t run_refine(Context& c) {
     KNNG_CUDA(cudaMemsetAsync(jc, 0, 8 * sizeof(unsigned long long), c.stream));
     auto join = [&](int mode, uint32_t lo, uint32_t hi, unsigned long long base, unsigned long long* out) {
         KNNG_DISPATCH_D(c.d, {
-            const size_t smem = JoinLayout<D>::bytes;
+            const size_t smem = JoinLayout<D>::bytes;  // (constexpr)
             auto kern = k_join<D>;
             KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-            kern<<<148, kJoinThreads, smem, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K, n,
+            kern<<<148 * 2, kJoinThreads, smem, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K, n,
                                                         mode, lo, hi, scount, soff, base, sfill, out, err,
                                                         mode == 0 ? jc : jc + 5);
         });
