@@ -17,9 +17,9 @@ the data path; the step time is the maximum over ranks.
 
 --impl reference times the reference's own CPU code (oracle/_ref, the
 reference headers compiled against a std::thread-pool stand-in for TBB) on the
-host cores: each step is one repetition of splitKmeansBinaryProcess over a
-bounded prefix of the same point set, scaled to a whole build (value =
-points / (t_rep * reps)).
+host cores: each step runs the same schedule -- every repetition of
+splitKmeansBinaryProcess, then every topUpSingle pass -- over a bounded prefix
+of the same point set (value = prefix points / step seconds).
 """
 from __future__ import annotations
 
@@ -43,8 +43,8 @@ DIM = 100
 K = 100
 MAX_LEAF = 1025        # buckets of at most 1024 points (leaf iff size < max_leaf)
 LLOYD_ITERS = 2
-REPS = 6
-REFINE = 0
+REPS = 3
+REFINE = 2
 SEED = 1
 QUERIES = 10_000
 FP32_NOMINAL_TFLOPS_AT_MAX_CLOCK = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4
@@ -172,10 +172,31 @@ def dist_done(world: int):
 
 # ------------------------------------------------------------ reference arm
 
-def reference_sample_rate(points: np.ndarray, reps_per_build: int, target_s: float, steps: int, warmup: int):
-    """Times the reference's splitKmeansBinaryProcess (one repetition, leaf <= 1024,
-    2 Lloyd iterations) on a prefix of the point set with all host threads.
-    Returns per-step points/s scaled to a whole build, the sample size and cores."""
+def reference_prefix(n: int, m: int) -> np.ndarray:
+    """The first m points of the benchmark point set (generated on the GPU when
+    one is present, as the GPU arm does; the set is randomly permuted, so a
+    prefix is a uniform sample)."""
+    from sigmod23ann_b200 import workloads
+
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            x = workloads.subspace_mixture_torch(n, seed=SEED)
+            out = x[:m].cpu().numpy().copy()
+            del x
+            torch.cuda.empty_cache()
+            return out
+    except Exception:
+        pass
+    return workloads.subspace_mixture(max(m, min(n, 1_000_000)), seed=SEED)[:m]
+
+
+def reference_sample_rate(n: int, reps: int, passes: int, target_s: float, steps: int, warmup: int):
+    """Times the reference's own code (all host threads) on a prefix of the
+    point set: each step = `reps` repetitions of splitKmeansBinaryProcess
+    (leaf <= 1024, 2 Lloyd iterations) then `passes` topUpSingle passes, from
+    empty sets.  The prefix is sized so one step takes about target_s."""
     from oracle import bindings
 
     cores = os.cpu_count() or 1
@@ -183,27 +204,29 @@ def reference_sample_rate(points: np.ndarray, reps_per_build: int, target_s: flo
     cores = int(os.environ["KNNG_REF_THREADS"])
     if not bindings.reference_available():
         return None
-    # Calibrate the prefix so one repetition takes about target_s seconds.
-    m = min(len(points), 100_000)
-    while True:
-        ref = bindings.ReferenceShim(points[:m], threaded=True)
+
+    def one_step(pts):
+        ref = bindings.ReferenceShim(pts, threaded=True)
         t = time.perf_counter()
-        ref.rep(LLOYD_ITERS, MAX_LEAF)
+        for _ in range(reps):
+            ref.rep(LLOYD_ITERS, MAX_LEAF)
+        for _ in range(passes):
+            ref.topup()
         dt = time.perf_counter() - t
         ref.close()
-        if dt >= target_s / 3 or m >= len(points):
+        return dt
+
+    m = min(n, 20_000)
+    pool = reference_prefix(n, min(n, 2_000_000))
+    while True:
+        dt = one_step(pool[:m])
+        if dt >= target_s / 2 or m >= len(pool):
             break
-        m = min(len(points), int(m * max(2.0, target_s / max(dt, 1e-3) * 0.8)))
-    ref = bindings.ReferenceShim(points[:m], threaded=True)
+        m = min(len(pool), int(m * min(8.0, max(1.5, target_s / max(dt, 1e-3)))))
+    sample = pool[:m]
     for _ in range(warmup):
-        ref.rep(LLOYD_ITERS, MAX_LEAF)
-    rates = []
-    for _ in range(steps):
-        t = time.perf_counter()
-        ref.rep(LLOYD_ITERS, MAX_LEAF)
-        dt = time.perf_counter() - t
-        rates.append(m / (dt * reps_per_build))
-    ref.close()
+        one_step(sample)
+    rates = [m / one_step(sample) for _ in range(steps)]
     return {"rates": rates, "sample_points": m, "cores": cores}
 
 
@@ -212,23 +235,20 @@ def run_reference(args):
     try:
         if rank != 0:
             return 0
-        from sigmod23ann_b200 import workloads
-
-        pts = workloads.subspace_mixture(min(args.n, 2_000_000), seed=SEED)
-        res = reference_sample_rate(pts, args.reps, args.cpu_seconds, args.steps, args.warmup)
+        res = reference_sample_rate(args.n, args.reps, args.refine, args.cpu_seconds, args.steps, args.warmup)
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (needs the reference sources)"}))
             return 0
         value = statistics.mean(res["rates"])
-        sample = (f"one repetition of the reference splitKmeansBinaryProcess (leaf<=1024, {LLOYD_ITERS} Lloyd "
-                  f"iterations) on the first {res['sample_points']:,} points of the seed-1 subspace mixture, "
-                  f"scaled to a {args.reps}-repetition build")
+        sample = (f"the reference's splitKmeansBinaryProcess x{args.reps} (leaf<=1024, {LLOYD_ITERS} Lloyd "
+                  f"iterations) then topUpSingle x{args.refine}, from empty sets, on the first "
+                  f"{res['sample_points']:,} points of the 10M seed-1 subspace mixture; points/s = sample / step time")
         line = {
             "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.n / value * 1000.0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "10M x 100 f32 subspace mixture, k=100, leaf<=1024 (sampled prefix on CPU)",
-                       "reps": args.reps, "lloyd_iters": LLOYD_ITERS},
+                       "reps": args.reps, "refine_passes": args.refine, "lloyd_iters": LLOYD_ITERS},
             "cpu_baseline": {"value": value, "unit": "points/s", "cores": res["cores"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -321,23 +341,38 @@ def run_ours(args):
 
     line = None
     if rank == 0:
-        per_launch_ms = leaf_ms / max(1, leaf_launches)
-        # Bucket kernel: the reference's unique-pair work, 3*d FLOPs per pair
-        # (d subtractions + d fused multiply-adds).
-        flops_per_launch = 3.0 * DIM * pairs / max(1, leaf_launches)
-        achieved = flops_per_launch / (per_launch_ms / 1000.0) / 1e12
-        roofline = {"bound": "fp32", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS_AT_MAX_CLOCK,
-                    "unit": "TFLOP/s", "frac": achieved / FP32_NOMINAL_TFLOPS_AT_MAX_CLOCK, "traffic": None,
-                    "kernel": "k_leaf (bucket all-pairs + set updates)",
-                    "peak_source": "nominal FP32 FMA rate, 148 SMs x 128 lanes x 2 x 1965 MHz (no measured FP32 peak)",
-                    "ms_per_launch": per_launch_ms, "share_of_step": leaf_ms / max(device_ms, 1e-9)}
+        last = stats_list[-1]
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except OSError:
+            pass
+        hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+        # Dominant kernel: the tensor-core join of the neighbour-of-neighbour
+        # pass.  Algorithmic bytes per launch: for every point q, the rows of
+        # R(q) and S(q) (4d bytes each) and the lists S(p) of R(q) (4k bytes
+        # each); sum_q |R(q)| = sum_q |S(q)| = n*k.
+        join_ms = sum(st["ms_refine_join"] for st in stats_list)
+        join_launches = sum(st["refine_join_launches"] for st in stats_list)
+        per_launch_ms = join_ms / max(1, join_launches)
+        bytes_per_launch = (2.0 * n * K * DIM * 4) + (1.0 * n * K * K * 4)
+        achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": achieved / hbm_peak, "traffic": None,
+                    "kernel": "k_join (neighbour-of-neighbour local join, tcgen05 TF32 filter)",
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)" if peaks else
+                                   "fallback 6650 GB/s",
+                    "ms_per_launch": per_launch_ms, "launches_per_step": join_launches / args.steps,
+                    "share_of_step": join_ms / max(device_ms, 1e-9),
+                    "algorithmic_bytes_per_launch": bytes_per_launch}
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{n:,} x {DIM} f32, 1024-cluster Zipf(1.1) 24-d subspace mixture (seed {SEED}), "
                                    f"k={K}, leaf<=1024, {args.reps} repetitions, {LLOYD_ITERS} Lloyd iterations, "
-                                   f"refine={args.refine}",
+                                   f"{args.refine} neighbour-of-neighbour passes",
                        "n": n, "k": K, "reps": args.reps, "parallelism": f"replicas x{world}",
                        "l2": "input 4 GB > 126 MB L2; no flush between steps"},
             "recall": rec, "recall_queries": len(q), "meets_recall_target": rec >= 0.94,
@@ -348,16 +383,13 @@ def run_ours(args):
     ctx.close()
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         try:
-            from sigmod23ann_b200 import workloads as wl
-
-            pts = wl.subspace_mixture(min(n, 2_000_000), seed=SEED)
-            res = reference_sample_rate(pts, args.reps, args.cpu_seconds, 1, 0)
+            res = reference_sample_rate(n, args.reps, args.refine, args.cpu_seconds, 1, 0)
             if res:
                 line["cpu_baseline"] = {
                     "value": res["rates"][0], "unit": "points/s", "cores": res["cores"], "kind": "reference",
-                    "sample": f"one repetition of the reference splitKmeansBinaryProcess on the first "
-                              f"{res['sample_points']:,} points (numpy copy of the same distribution), "
-                              f"scaled to a {args.reps}-repetition build"}
+                    "sample": f"the reference's splitKmeansBinaryProcess x{args.reps} then topUpSingle x{args.refine} "
+                              f"(std::thread-pool TBB stand-in, all host threads) on the first "
+                              f"{res['sample_points']:,} points of the same point set; points/s = sample / seconds"}
         except Exception as e:  # the baseline must not hide the GPU number
             line["cpu_baseline"] = {"error": str(e)}
     if rank == 0:

@@ -89,7 +89,7 @@ typedef struct knng_stats {
     uint64_t leaf_launches;   /* bucket-kernel launches */
     uint64_t kernel_launches; /* all kernels launched by the call */
     uint64_t refine_changed;  /* points whose set changed in the refinement pass */
-    double ms_refine_join;    /* refinement: reverse lists + tensor-core join */
+    double ms_refine_join;    /* refinement: tensor-core join kernels */
     double ms_refine_apply;   /* refinement: sorted replay of survivors */
     double ms_refine_fallback;/* refinement: unused by the join (0) */
     uint64_t refine_pairs;    /* (point, candidate) pairs the join evaluated */
@@ -98,6 +98,8 @@ typedef struct knng_stats {
     uint64_t refine_exact;    /* exact FP32 distances computed by the join */
     uint64_t refine_emits;    /* survivor records written (before de-duplication) */
     uint64_t refine_overflow; /* store rounds the join needed (survivor memory cap) */
+    double ms_refine_prep;    /* refinement: snapshot, reverse lists, scans */
+    uint64_t refine_join_launches; /* join-kernel launches (counting + store rounds) */
 } knng_stats;
 
 /* Fills the reference's parameters: k=100, max_leaf=200, max_leaf_odd=400,

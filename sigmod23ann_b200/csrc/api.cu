@@ -422,6 +422,8 @@ void add_refine_stats(knng_stats* stats, const Context& c, uint64_t changed, dou
     stats->refine_exact += c.last_refine.exact;
     stats->refine_emits += c.last_refine.emits;
     stats->refine_overflow += c.last_refine.overflow;
+    stats->ms_refine_prep += c.last_refine.ms_prep;
+    stats->refine_join_launches += c.last_refine.join_launches;
 }
 
 void validate_params(const knng_params* p) {

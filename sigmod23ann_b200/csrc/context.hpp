@@ -69,8 +69,8 @@ struct Context {
     int refine_mode = 0;
     // Breakdown of the last refinement pass.
     struct RefineRecord {
-        double ms_join = 0, ms_apply = 0, ms_fallback = 0;
-        uint64_t pairs = 0, filter_pass = 0, member_skip = 0, exact = 0, emits = 0, overflow = 0;
+        double ms_join = 0, ms_apply = 0, ms_fallback = 0, ms_prep = 0;
+        uint64_t pairs = 0, filter_pass = 0, member_skip = 0, exact = 0, emits = 0, overflow = 0, join_launches = 0;
     } last_refine;
 };
 

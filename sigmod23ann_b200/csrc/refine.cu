@@ -902,7 +902,12 @@ uint64_t run_refine(Context& c) {
     KNNG_CUDA(cudaMemsetAsync(scount, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
     KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
     KNNG_CUDA(cudaMemsetAsync(jc, 0, 8 * sizeof(unsigned long long), c.stream));
+    float ms_join_kernels = 0.f;
     auto join = [&](int mode, uint32_t lo, uint32_t hi, unsigned long long base, unsigned long long* out) {
+        cudaEvent_t j0, j1;
+        KNNG_CUDA(cudaEventCreate(&j0));
+        KNNG_CUDA(cudaEventCreate(&j1));
+        KNNG_CUDA(cudaEventRecord(j0, c.stream));
         KNNG_DISPATCH_D(c.d, {
             const size_t smem = JoinLayout<D>::bytes;  // (constexpr)
             auto kern = k_join<D>;
@@ -912,7 +917,15 @@ uint64_t run_refine(Context& c) {
                                                         mode == 0 ? jc : jc + 5);
         });
         ++c.launches;
+        ++rec.join_launches;
         KNNG_CUDA(cudaGetLastError());
+        KNNG_CUDA(cudaEventRecord(j1, c.stream));
+        KNNG_CUDA(cudaEventSynchronize(j1));
+        float ms = 0.f;
+        KNNG_CUDA(cudaEventElapsedTime(&ms, j0, j1));
+        ms_join_kernels += ms;
+        cudaEventDestroy(j0);
+        cudaEventDestroy(j1);
     };
     join(0, 0, n, 0, nullptr);
     device_scan(c, scount, n, soff);
@@ -1007,7 +1020,8 @@ uint64_t run_refine(Context& c) {
     float ms_count = 0;
     KNNG_CUDA(cudaEventElapsedTime(&ms_count, ev[0], ev[1]));
     for (auto& e : ev) cudaEventDestroy(e);
-    rec.ms_join = ms_count + ms_join;
+    rec.ms_join = ms_join_kernels;
+    rec.ms_prep = ms_count + ms_join - ms_join_kernels;
     rec.ms_apply = ms_apply;
     rec.ms_fallback = 0;
     rec.pairs = hc[0];
