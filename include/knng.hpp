@@ -1,0 +1,62 @@
+// knng.hpp -- header-only C++ convenience over the C ABI in knng.h.
+//
+// constructResult() has the signature of the reference's entry point
+// SolutionKmeans::constructResult(float points[][112], uint32_t numPoints,
+// vector<vector<uint32_t>>& result) (src/SolutionKmeans.hpp:558), so a caller
+// of the reference can switch by changing one call.  Errors are reported as
+// std::runtime_error (the ABI itself never throws).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "knng.h"
+
+namespace knng_b200 {
+
+class Context {
+public:
+    explicit Context(int device = 0, uint64_t hbm_budget_bytes = 0) {
+        check(knng_create(device, hbm_budget_bytes, &ctx_), nullptr);
+    }
+    ~Context() {
+        if (ctx_) knng_destroy(ctx_);
+    }
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+    knng_context* get() const { return ctx_; }
+
+    static void check(knng_status s, knng_context* ctx) {
+        if (s == KNNG_OK) return;
+        std::string msg = knng_status_string(s);
+        if (ctx) {
+            const char* e = knng_last_error(ctx);
+            if (e && *e) msg += std::string(": ") + e;
+        }
+        throw std::runtime_error("knng: " + msg);
+    }
+
+private:
+    knng_context* ctx_ = nullptr;
+};
+
+// Rows of `stride` floats (the reference uses 112), first `dims` used.
+template <int Stride>
+void constructResult(float points[][Stride], uint32_t numPoints, std::vector<std::vector<uint32_t>>& result,
+                     const knng_params* params = nullptr, uint32_t dims = 100, int device = 0) {
+    knng_params p;
+    knng_default_params(&p);
+    if (params) p = *params;
+    Context ctx(device);
+    std::vector<uint32_t> ids(static_cast<size_t>(numPoints) * p.k);
+    Context::check(knng_build(ctx.get(), &points[0][0], numPoints, dims, sizeof(float) * Stride, &p, ids.data(), nullptr,
+                              nullptr),
+                   ctx.get());
+    result.resize(numPoints);
+    for (uint32_t i = 0; i < numPoints; ++i)
+        result[i].assign(ids.begin() + static_cast<size_t>(i) * p.k, ids.begin() + static_cast<size_t>(i + 1) * p.k);
+}
+
+}  // namespace knng_b200

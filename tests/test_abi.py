@@ -58,3 +58,40 @@ def test_create_without_device_reports_no_device(knng_lib):
     with pytest.raises(api.KnngError) as e:
         api.KnngContext(0)
     assert e.value.status == 7
+
+
+def test_cpp_wrapper_compiles_links_and_reports_no_device(knng_lib, tmp_path):
+    """A C++ caller of the reference's shape (float[][112] rows) builds against
+    include/knng.hpp and libknng.so; without a GPU the wrapper throws with
+    KNNG_ERR_NO_DEVICE's message."""
+    import subprocess
+
+    import torch
+
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <cstdlib>
+#include "knng.hpp"
+static float pts[4][112];
+int main() {
+    std::vector<std::vector<uint32_t>> result;
+    try {
+        knng_b200::constructResult(pts, 4, result);
+    } catch (const std::runtime_error& e) {
+        std::printf("%s\n", e.what());
+        return 3;
+    }
+    std::printf("rows %zu\n", result.size());
+    return result.size() == 4 ? 0 : 1;
+}
+''')
+    exe = tmp_path / "caller"
+    libdir = os.path.join(ROOT, "sigmod23ann_b200")
+    subprocess.run(["/usr/bin/g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    f"-L{libdir}", "-lknng", f"-Wl,-rpath,{libdir}"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    if torch.cuda.is_available():
+        assert r.returncode == 0, r.stdout + r.stderr
+    else:
+        assert r.returncode == 3 and "no sm_100" in r.stdout, r.stdout + r.stderr
