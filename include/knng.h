@@ -212,6 +212,34 @@ knng_status knng_finalize(knng_context* ctx, uint32_t* out_ids, float* out_dists
 knng_status knng_debug_tile_gram(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n,
                                  uint32_t d, float* out);
 
+/* ------------------------------------------------------ allocation-free pass
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory during the call (code running inside another framework's memory pool
+ * or under a hard memory cap, or holding only device pointers handed over by a
+ * host application): the neighbour-of-neighbour pass of knng_refine, one warp
+ * per point, on buffers the caller owns, allocating nothing.
+ *
+ *   d_points   n x d float32, rows packed (stride 4*d bytes), 16-byte aligned
+ *   d_snapshot n x k uint32, written (each set's ids, sorted)
+ *   d_dist, d_ids (n x k), d_size, d_maxslot, d_bound (n): the sets, in the
+ *              layout of knng_get_sets; updated in place
+ *   d_changed  one uint32, written: points whose set changed
+ *   stream     cudaStream_t to run on (NULL: the default stream)
+ * All pointers are device pointers on the current device.  The call is
+ * asynchronous on `stream`.
+ *
+ * Its scratch is a fixed 4 MiB device array (32 regions of 16,384 records)
+ * that every GPU loading the library keeps until the process exits; k is
+ * limited to k*k <= 16,384 (k <= 128), larger k is rejected with
+ * KNNG_ERR_UNSUPPORTED.  The first call on a device looks up that array's
+ * device address; make it before capturing the call into a CUDA graph.  Every
+ * call shares the array: calls that overlap on the GPU (different streams, or
+ * devices sharing a context) race, so serialise them.  No state carries over
+ * between calls. */
+knng_status knng_refine_pointwise_noalloc(const float* d_points, uint32_t n, uint32_t d, uint32_t k,
+                                          uint32_t* d_snapshot, float* d_dist, uint32_t* d_ids, uint32_t* d_size,
+                                          uint32_t* d_maxslot, float* d_bound, uint32_t* d_changed, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,7 +32,7 @@ EXPORTED = [
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
-    "knng_debug_tile_gram",
+    "knng_debug_tile_gram", "knng_refine_pointwise_noalloc",
 ]
 
 
@@ -104,6 +104,7 @@ def load_library(path: str = LIB_PATH):
         "knng_set_sets": (c_int, [P, P, P, P, P, P]),
         "knng_finalize": (c_int, [P, P, P]),
         "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
+        "knng_refine_pointwise_noalloc": (c_int, [P, c_uint32, c_uint32, c_uint32, P, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

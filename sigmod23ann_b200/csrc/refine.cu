@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "context.hpp"
@@ -1034,3 +1035,83 @@ uint64_t run_refine(Context& c) {
 }
 
 }  // namespace knng
+
+// ------------------------------------------------------------------------
+// Allocation-free neighbour-of-neighbour pass.
+//
+// Some callers cannot allocate device memory while they call into this
+// library: code that runs inside another framework's memory pool or under a
+// strict memory budget, code that only receives device pointers from a host
+// application, and code paths where a cudaMalloc would synchronise the device
+// at the wrong moment.  knng_refine_pointwise_noalloc serves them: it runs the
+// one-warp-per-point pass on buffers the caller passes in, and keeps its only
+// scratch -- each warp's survivor records -- in the fixed device array below,
+// which every GPU that loads the library holds until the process exits.
+namespace {
+
+constexpr uint32_t kNoAllocWarps = 32;                 // warps of the launch; one scratch region each
+constexpr uint32_t kNoAllocRegion = 16384;             // records per region: >= k*k for every k <= 128
+static __device__ __align__(256) unsigned long long g_noalloc_survivors[kNoAllocWarps * kNoAllocRegion];  // 4 MiB
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, resolved once per
+// device (the array's name in host code is a host-side stand-in, not a device
+// address).
+cudaError_t noalloc_scratch(unsigned long long** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_survivors);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[dev] = p;
+    }
+    *out = static_cast<unsigned long long*>(g_noalloc_addr[dev]);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" knng_status knng_refine_pointwise_noalloc(const float* d_points, uint32_t n, uint32_t d, uint32_t k,
+                                                     uint32_t* d_snapshot, float* d_dist, uint32_t* d_ids,
+                                                     uint32_t* d_size, uint32_t* d_maxslot, float* d_bound,
+                                                     uint32_t* d_changed, void* stream) {
+    using namespace knng;
+    // A point has at most k*k candidates; a scratch region holds kNoAllocRegion.
+    if (k == 0 || static_cast<uint64_t>(k) * k > kNoAllocRegion) return KNNG_ERR_UNSUPPORTED;
+    if (!dim_supported(d)) return KNNG_ERR_UNSUPPORTED;
+    if (n == 0) return KNNG_OK;
+    if (!d_points || !d_snapshot || !d_dist || !d_ids || !d_size || !d_maxslot || !d_bound || !d_changed)
+        return KNNG_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(d_points) % 16 != 0) return KNNG_ERR_INVALID_ARGUMENT;
+    unsigned long long* scratch_keys = nullptr;
+    if (noalloc_scratch(&scratch_keys) != cudaSuccess) {
+        cudaGetLastError();
+        return KNNG_ERR_CUDA;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int K = static_cast<int>(k);
+    if (cudaMemsetAsync(d_changed, 0, sizeof(uint32_t), s) != cudaSuccess) {
+        cudaGetLastError();
+        return KNNG_ERR_CUDA;
+    }
+    const uint32_t sblocks = std::min<uint32_t>((n + kSnapWarps - 1) / kSnapWarps, 148 * 8);
+    k_snapshot<<<sblocks, kSnapWarps * kWarp, 0, s>>>(d_ids, n, K, d_snapshot);
+    try {
+        KNNG_DISPATCH_D(d, {
+            k_refine<D><<<kNoAllocWarps / kRefWarps, kRefWarps * kWarp, 0, s>>>(
+                d_snapshot, d_points, static_cast<int>(d), d_dist, d_ids, d_size, d_maxslot, d_bound, K, n, nullptr,
+                scratch_keys, kNoAllocRegion, d_changed);
+        });
+    } catch (const Error& e) {
+        return e.status;
+    }
+    if (cudaGetLastError() != cudaSuccess) return KNNG_ERR_CUDA;
+    return KNNG_OK;
+}
