@@ -54,6 +54,16 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objects):
         subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objects, "-ccbin", "/usr/bin/g++"], check=True)
+    # Command-line tools: the reference's program shape (contest file in,
+    # output.bin out) and its grader.
+    for name, link in (("knng_build", True), ("knng_grade", False)):
+        src = os.path.join(HERE, "cli", name + ".cpp")
+        exe = os.path.join(HERE, "cli", name)
+        if force or _stale(exe, [src, LIB] if link else [src]):
+            cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-I", INCLUDE, src, "-o", exe]
+            if link:
+                cmd += [f"-L{HERE}", "-lknng", f"-Wl,-rpath,{HERE}"]
+            subprocess.run(cmd, check=True)
     return LIB
 
 

@@ -1,0 +1,65 @@
+// knng_build -- the reference's command line (src/main.cpp:39-71) on the GPU:
+//
+//   knng_build [input.bin] [output.bin] [reps] [refine passes] [max_leaf]
+//
+// input.bin: uint32 N, then N rows of 100 float32 (the contest format read by
+// ReadBinArray, src/io.h:66-95).  output.bin: N rows of 100 uint32 neighbour
+// ids, sorted by distance, no header (SaveKNNG, src/io.h:21-33).  Defaults:
+// dummy-data.bin, output.bin, the reference's parameters (knng_default_params).
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "knng.h"
+
+int main(int argc, char** argv) {
+    const std::string in = argc > 1 ? argv[1] : "dummy-data.bin";
+    const std::string out = argc > 2 ? argv[2] : "output.bin";
+    knng_params p;
+    knng_default_params(&p);
+    if (argc > 3) p.reps = static_cast<uint32_t>(std::atoi(argv[3]));
+    if (argc > 4) p.refine = static_cast<uint32_t>(std::atoi(argv[4]));
+    if (argc > 5) {
+        p.max_leaf = static_cast<uint32_t>(std::atoi(argv[5]));
+        p.max_leaf_odd = 0;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    std::ifstream f(in, std::ios::binary);
+    if (!f) {
+        std::fprintf(stderr, "cannot open %s\n", in.c_str());
+        return 2;
+    }
+    uint32_t n = 0;
+    f.read(reinterpret_cast<char*>(&n), sizeof(n));
+    std::vector<float> pts(static_cast<size_t>(n) * 100);
+    f.read(reinterpret_cast<char*>(pts.data()), static_cast<std::streamsize>(pts.size() * sizeof(float)));
+    if (!f) {
+        std::fprintf(stderr, "%s: expected %u rows of 100 float32\n", in.c_str(), n);
+        return 2;
+    }
+    knng_context* ctx = nullptr;
+    knng_status s = knng_create(0, 0, &ctx);
+    if (s != KNNG_OK) {
+        std::fprintf(stderr, "knng_create: %s\n", knng_status_string(s));
+        return 3;
+    }
+    std::vector<uint32_t> ids(static_cast<size_t>(n) * p.k);
+    knng_stats st;
+    s = knng_build(ctx, pts.data(), n, 100, 400, &p, ids.data(), nullptr, &st);
+    if (s != KNNG_OK) {
+        std::fprintf(stderr, "knng_build: %s: %s\n", knng_status_string(s), knng_last_error(ctx));
+        knng_destroy(ctx);
+        return 3;
+    }
+    knng_destroy(ctx);
+    std::ofstream o(out, std::ios::binary);
+    o.write(reinterpret_cast<const char*>(ids.data()), static_cast<std::streamsize>(ids.size() * sizeof(uint32_t)));
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("points %u  reps %u  refine passes %u  device ms %.1f  total ms %.1f  -> %s\n", n, p.reps, p.refine,
+                st.ms_total + st.ms_finalize, ms, out.c_str());
+    return 0;
+}
