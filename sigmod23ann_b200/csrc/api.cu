@@ -63,7 +63,8 @@ void* scratch(Context& c, const char* name, size_t bytes) {
         if (e.first == name) {
             if (e.second.bytes >= bytes) return e.second.ptr;
             KNNG_CUDA(cudaStreamSynchronize(c.stream));
-            const size_t grown = std::max(bytes, e.second.bytes * 3 / 2);
+            size_t grown = std::max(bytes, e.second.bytes * 3 / 2);
+            if (c.held - e.second.bytes + grown > c.budget) grown = bytes;
             dev_free(c, e.second.ptr, e.second.bytes);
             e.second.ptr = nullptr;
             e.second.bytes = 0;
@@ -77,6 +78,12 @@ void* scratch(Context& c, const char* name, size_t bytes) {
     b.bytes = bytes == 0 ? 16 : bytes;
     c.scratch.emplace_back(name, b);
     return b.ptr;
+}
+
+size_t scratch_bytes(const Context& c, const char* name) {
+    for (const auto& e : c.scratch)
+        if (e.first == name) return e.second.bytes;
+    return 0;
 }
 
 namespace {
@@ -530,6 +537,8 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     if (!c) return KNNG_ERR_OUT_OF_MEMORY;
     c->device = device;
     if (const char* r = std::getenv("KNNG_REFINE")) c->refine_mode = std::strcmp(r, "pointwise") == 0 ? 1 : 0;
+    if (const char* r = std::getenv("KNNG_REFINE_SLOTS")) c->refine_slots = std::max(0, std::atoi(r));
+    if (const char* r = std::getenv("KNNG_REFINE_ROUND")) c->refine_round = std::strtoull(r, nullptr, 10);
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;

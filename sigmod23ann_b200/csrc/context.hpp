@@ -67,6 +67,13 @@ struct Context {
     // Neighbour-of-neighbour pass: 0 = local join on the tensor cores,
     // 1 = one warp per point (environment KNNG_REFINE=pointwise at creation).
     int refine_mode = 0;
+    // Survivor slots per point in the join's direct pass: -1 = sized from the
+    // free budget (environment KNNG_REFINE_SLOTS at creation overrides it,
+    // 0 = every point through the overflow rounds).
+    int refine_slots = -1;
+    // Records per overflow round: 0 = sized from the free budget (environment
+    // KNNG_REFINE_ROUND at creation overrides it).
+    uint64_t refine_round = 0;
     // Breakdown of the last refinement pass.
     struct RefineRecord {
         double ms_join = 0, ms_apply = 0, ms_fallback = 0, ms_prep = 0;
@@ -78,6 +85,8 @@ struct Context {
 void* dev_alloc(Context& c, size_t bytes);
 void dev_free(Context& c, void* p, size_t bytes);
 void* scratch(Context& c, const char* name, size_t bytes);
+// Bytes currently held by the named scratch allocation (0 if none).
+size_t scratch_bytes(const Context& c, const char* name);
 void release_all(Context& c);
 
 // Uploads `count` elements into named scratch and returns the device pointer.

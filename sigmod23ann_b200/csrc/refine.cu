@@ -387,14 +387,16 @@ __device__ __forceinline__ void stage_rows(float* __restrict__ dst, const uint32
 }
 
 
-// mode 0 counts survivors per point into surv_count; mode 1 writes them at
-// surv[surv_off[p] - base + cursor] for points p in [p_lo, p_hi).
+// mode 0 (direct): counts every point's survivors exactly into surv_count and
+// writes the first `slots` of them at surv[p * slots + cursor].
+// mode 1 (overflow): for points p in [p_lo, p_hi) with surv_count[p] > slots,
+// writes all survivors at surv[surv_off[p] - base + cursor].
 template <int D>
 __global__ void __launch_bounds__(kJoinThreads, 2)
     k_join(const uint32_t* __restrict__ snap, const unsigned long long* __restrict__ rev_off,
            const uint32_t* __restrict__ rev, const float* __restrict__ pts, int ld, const float* __restrict__ bound,
-           const uint32_t* __restrict__ set_size, int K, uint32_t n, int mode, uint32_t p_lo, uint32_t p_hi,
-           uint32_t* __restrict__ surv_count, const unsigned long long* __restrict__ surv_off,
+           const uint32_t* __restrict__ set_size, int K, uint32_t n, int mode, uint32_t slots, uint32_t p_lo,
+           uint32_t p_hi, uint32_t* __restrict__ surv_count, const unsigned long long* __restrict__ surv_off,
            unsigned long long surv_base, uint32_t* __restrict__ surv_fill, unsigned long long* __restrict__ surv,
            uint32_t* __restrict__ error_flag, unsigned long long* __restrict__ counters) {
     using L = JoinLayout<D>;
@@ -466,7 +468,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
             bool any = false;
             if (tid < kTile) {
                 uint32_t p = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
-                if (p != kNone && (p < p_lo || p >= p_hi)) p = kNone;
+                if (p != kNone && (p < p_lo || p >= p_hi || (mode == 1 && surv_count[p] <= slots))) p = kNone;
                 pid[tid] = p;
                 bnd[tid] = p != kNone ? bound[p] : 0.0f;
                 // A set that is not full lists its empty slots as id 0.
@@ -639,15 +641,17 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                     const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(Bo + j * D), prow);
                     if (d < bp) {
                         ++n_emit;
+                        const unsigned long long rec =
+                            (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
                         if (mode == 0) {
-                            atomicAdd(&surv_count[p], 1u);
+                            const uint32_t s = atomicAdd(&surv_count[p], 1u);
+                            if (s < slots) surv[static_cast<size_t>(p) * slots + s] = rec;
                         } else {
                             const uint32_t s2 = atomicAdd(&surv_fill[p], 1u);
-                            // The store pass repeats the counting pass exactly; the
+                            // The overflow pass repeats the direct pass exactly; the
                             // guard keeps a disagreement from writing past p's range.
                             if (s2 < surv_count[p])
-                                surv[surv_off[p] - surv_base + s2] =
-                                    (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
+                                surv[surv_off[p] - surv_base + s2] = rec;
                             else
                                 atomicExch(error_flag, 2u);
                         }
@@ -701,26 +705,32 @@ __device__ __forceinline__ uint32_t replay_sorted(unsigned long long* buf, uint3
 
 constexpr int kApplyCap = 1024;  // survivors sorted in shared memory per warp
 
-// Points in [p_lo, p_hi): survivors at surv[surv_off[p] - base ...], sorted in
-// shared memory when they fit; larger lists are queued on `big`.
+// Points in [p_lo, p_hi). With stride > 0 (direct slots): points with at
+// most `stride` survivors, read at surv[p * stride ...]. With stride == 0
+// (overflow rounds): points with more than `skip_upto` survivors, read at
+// surv[surv_off[p] - base ...]. Lists are sorted in shared memory when they
+// fit; larger lists are queued on `big`.
 __global__ void __launch_bounds__(kRefWarps * kWarp)
     k_apply(uint32_t p_lo, uint32_t p_hi, int K, const uint32_t* __restrict__ surv_count,
             const unsigned long long* __restrict__ surv_off, unsigned long long surv_base,
-            const unsigned long long* __restrict__ surv, float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
-            uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound,
-            uint32_t* __restrict__ big, uint32_t* __restrict__ big_n, uint32_t* __restrict__ changed_count) {
+            const unsigned long long* __restrict__ surv, uint32_t stride, uint32_t skip_upto,
+            float* __restrict__ set_dist, uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size,
+            uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound, uint32_t* __restrict__ big,
+            uint32_t* __restrict__ big_n, uint32_t* __restrict__ changed_count) {
     __shared__ unsigned long long keys_s[kRefWarps][kApplyCap];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     unsigned long long* buf = keys_s[warp];
     for (uint32_t p = p_lo + blockIdx.x * kRefWarps + warp; p < p_hi; p += gridDim.x * kRefWarps) {
         const uint32_t S = surv_count[p];
         if (S == 0) continue;
+        if (stride ? S > stride : S <= skip_upto) continue;
         if (S > kApplyCap) {
             if (lane == 0) big[atomicAdd(big_n, 1u)] = p;
             continue;
         }
         const uint32_t P2 = pow2_at_least(S);
-        const unsigned long long* src = surv + (surv_off[p] - surv_base);
+        const unsigned long long* src =
+            stride ? surv + static_cast<size_t>(p) * stride : surv + (surv_off[p] - surv_base);
         for (uint32_t t = lane; t < P2; t += kWarp) buf[t] = t < S ? src[t] : ~0ull;
         const uint32_t ch = replay_sorted(buf, S, P2, p, K, set_dist, set_id, set_size, set_maxslot, set_bound, lane);
         if (ch && lane == 0) atomicAdd(changed_count, 1u);
@@ -822,8 +832,23 @@ void device_scan(Context& c, const uint32_t* in, uint64_t n, unsigned long long*
     KNNG_CUDA(cudaGetLastError());
 }
 
-// Survivor records (8 bytes each) held at once by one store round.
-constexpr uint64_t kMaxRoundRecords = 1ull << 31;
+// Points with more survivors than their direct slots are stored in rounds of
+// at least this many records (8 bytes each), more when the budget allows.
+constexpr uint64_t kMinRoundRecords = 1ull << 24;
+
+// ocount[p] = count[p] when it exceeds `slots`, else 0; *max_count = the
+// largest count.
+__global__ void k_overflow_counts(const uint32_t* __restrict__ count, uint32_t n, uint32_t slots,
+                                  uint32_t* __restrict__ ocount, uint32_t* __restrict__ max_count) {
+    uint32_t m = 0;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t v = count[p];
+        ocount[p] = v > slots ? v : 0u;
+        m = max(m, v);
+    }
+    for (int o = kWarp / 2; o > 0; o /= 2) m = max(m, __shfl_xor_sync(kFull, m, o));
+    if ((threadIdx.x % kWarp) == 0 && m) atomicMax(max_count, m);
+}
 
 }  // namespace
 
@@ -893,17 +918,38 @@ uint64_t run_refine(Context& c) {
     c.launches += 2;
     KNNG_CUDA(cudaGetLastError());
 
-    // Join, counting pass: survivors per point.
+    // Join, direct pass: exact survivor counts, and the survivors of every point
+    // with at most `slots` of them in fixed per-point slots.
     auto* scount = static_cast<uint32_t*>(scratch(c, "surv_count", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* ocount = static_cast<uint32_t*>(scratch(c, "surv_ovf_count", static_cast<size_t>(n) * sizeof(uint32_t)));
     auto* sfill = static_cast<uint32_t*>(scratch(c, "surv_fill", static_cast<size_t>(n) * sizeof(uint32_t)));
     auto* soff = static_cast<unsigned long long*>(
         scratch(c, "surv_offsets", (static_cast<size_t>(n) + 1) * sizeof(unsigned long long)));
     auto* err = static_cast<uint32_t*>(scratch(c, "join_error", sizeof(uint32_t)));
-    auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 8 * sizeof(unsigned long long)));
+    auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 16 * sizeof(unsigned long long)));
+    auto* counters = static_cast<uint32_t*>(scratch(c, "apply_counters", 4 * sizeof(uint32_t)));
+    auto* big = static_cast<uint32_t*>(scratch(c, "apply_big", static_cast<size_t>(n) * sizeof(uint32_t)));
     KNNG_CUDA(cudaMemsetAsync(scount, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
     KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
-    KNNG_CUDA(cudaMemsetAsync(jc, 0, 8 * sizeof(unsigned long long), c.stream));
-    float ms_join_kernels = 0.f;
+    KNNG_CUDA(cudaMemsetAsync(jc, 0, 16 * sizeof(unsigned long long), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), c.stream));
+    uint32_t slots = 0;
+    if (c.refine_slots >= 0) {
+        slots = std::min<uint32_t>(static_cast<uint32_t>(c.refine_slots), kApplyCap);
+    } else {
+        // Half of what the budget leaves free (counting the slots already held),
+        // after a reserve for the overflow rounds.
+        const uint64_t held_other = c.held - scratch_bytes(c, "surv_direct");
+        const uint64_t reserve = (1ull << 30) + kMinRoundRecords * 8;
+        const uint64_t avail = c.budget > held_other + reserve ? (c.budget - held_other - reserve) / 2 : 0;
+        slots = static_cast<uint32_t>(std::min<uint64_t>(kApplyCap, avail / (static_cast<uint64_t>(n) * 8)));
+        if (slots < 8) slots = 0;
+    }
+    unsigned long long* direct =
+        slots ? static_cast<unsigned long long*>(
+                    scratch(c, "surv_direct", static_cast<size_t>(n) * slots * sizeof(unsigned long long)))
+              : nullptr;
+    float ms_join_kernels = 0.f, ms_ovf_kernels = 0.f;
     auto join = [&](int mode, uint32_t lo, uint32_t hi, unsigned long long base, unsigned long long* out) {
         cudaEvent_t j0, j1;
         KNNG_CUDA(cudaEventCreate(&j0));
@@ -914,117 +960,145 @@ uint64_t run_refine(Context& c) {
             auto kern = k_join<D>;
             KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
             kern<<<148 * 2, kJoinThreads, smem, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K, n,
-                                                        mode, lo, hi, scount, soff, base, sfill, out, err,
-                                                        mode == 0 ? jc : jc + 5);
+                                                        mode, slots, lo, hi, scount, soff, base, sfill, out, err,
+                                                        mode == 0 ? jc : jc + 8);
         });
         ++c.launches;
-        ++rec.join_launches;
+        if (mode == 0) ++rec.join_launches;
         KNNG_CUDA(cudaGetLastError());
         KNNG_CUDA(cudaEventRecord(j1, c.stream));
         KNNG_CUDA(cudaEventSynchronize(j1));
         float ms = 0.f;
         KNNG_CUDA(cudaEventElapsedTime(&ms, j0, j1));
-        ms_join_kernels += ms;
+        (mode == 0 ? ms_join_kernels : ms_ovf_kernels) += ms;
         cudaEventDestroy(j0);
         cudaEventDestroy(j1);
     };
-    join(0, 0, n, 0, nullptr);
-    device_scan(c, scount, n, soff);
-    // Store rounds over point ranges whose records fit kMaxRoundRecords.
-    std::vector<unsigned long long> hoff(static_cast<size_t>(n) + 1);
-    download(c, hoff.data(), soff, hoff.size());
+    auto apply = [&](uint32_t lo, uint32_t hi, const unsigned long long* src, uint32_t stride, unsigned long long base,
+                     unsigned long long* big_keys, uint32_t big_cap) {
+        KNNG_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t), c.stream));
+        const uint32_t ablocks = std::max<uint32_t>(1, std::min<uint32_t>((hi - lo + kRefWarps - 1) / kRefWarps, 148 * 16));
+        k_apply<<<ablocks, kRefWarps * kWarp, 0, c.stream>>>(lo, hi, K, scount, soff, base, src, stride, slots,
+                                                             c.set_dist, c.set_id, c.set_size, c.set_maxslot,
+                                                             c.set_bound, big, counters, counters + 1);
+        ++c.launches;
+        if (big_keys) {
+            k_apply_big<<<148 * 2, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, soff, base, src, big_keys,
+                                                                    big_cap, c.set_dist, c.set_id, c.set_size,
+                                                                    c.set_maxslot, c.set_bound, counters + 1);
+            ++c.launches;
+        }
+        KNNG_CUDA(cudaGetLastError());
+    };
+    auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+        float ms = 0.f;
+        KNNG_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return ms;
+    };
+    KNNG_CUDA(cudaEventRecord(ev[1], c.stream));
+    join(0, 0, n, 0, direct);
+    cudaEvent_t a0, a1;
+    KNNG_CUDA(cudaEventCreate(&a0));
+    KNNG_CUDA(cudaEventCreate(&a1));
+    KNNG_CUDA(cudaEventRecord(a0, c.stream));
+    if (slots) apply(0, n, direct, slots, 0, nullptr, 0);
+    KNNG_CUDA(cudaEventRecord(a1, c.stream));
+    // Points whose survivors overflowed their slots: CSR offsets over them alone.
+    const uint32_t oblocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 255) / 256, 148 * 8));
+    k_overflow_counts<<<oblocks, 256, 0, c.stream>>>(scount, n, slots, ocount, counters + 2);
+    ++c.launches;
+    KNNG_CUDA(cudaGetLastError());
+    device_scan(c, ocount, n, soff);
+    unsigned long long total = 0;
+    uint32_t hc32[4] = {0, 0, 0, 0};
+    download(c, &total, soff + n, 1);
+    download(c, hc32, counters, 4);
     uint32_t herr = 0;
     download(c, &herr, err, 1);
+    float ms_apply = elapsed(a0, a1);
+    cudaEventDestroy(a0);
+    cudaEventDestroy(a1);
     if (herr) {
         for (auto& e : ev) cudaEventDestroy(e);
         fail(KNNG_ERR_CUDA, "tensor-core join: an MMA completion wait timed out");
     }
-    const unsigned long long total = hoff[n];
-    unsigned long long round_cap = std::min<unsigned long long>(total, kMaxRoundRecords);
-    auto* surv = static_cast<unsigned long long*>(scratch(c, "surv_keys", (round_cap + 1) * sizeof(unsigned long long)));
-    uint32_t max_count = 0;
-    for (uint32_t i = 0; i < n; ++i) max_count = std::max<uint32_t>(max_count, static_cast<uint32_t>(hoff[i + 1] - hoff[i]));
-    auto* big = static_cast<uint32_t*>(scratch(c, "apply_big", static_cast<size_t>(n) * sizeof(uint32_t)));
-    auto* counters = static_cast<uint32_t*>(scratch(c, "apply_counters", 2 * sizeof(uint32_t)));
-    KNNG_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(uint32_t), c.stream));
-    const uint32_t big_cap = pow2_at_least(std::max<uint32_t>(max_count, 2));
-    const uint32_t big_blocks = 148 * 2;
-    unsigned long long* big_keys = nullptr;
-    if (max_count > static_cast<uint32_t>(kApplyCap))
-        big_keys = static_cast<unsigned long long*>(
-            scratch(c, "apply_big_keys", static_cast<size_t>(big_blocks) * kRefWarps * big_cap * sizeof(unsigned long long)));
-    float ms_join = 0, ms_apply = 0;
-    KNNG_CUDA(cudaEventRecord(ev[1], c.stream));
-    uint32_t lo = 0;
-    while (lo < n) {
-        uint32_t hi = lo + 1;
-        // Largest hi with hoff[hi] - hoff[lo] <= round_cap (at least one point).
-        uint32_t a = lo + 1, b = n;
-        while (a < b) {
-            const uint32_t mid = a + (b - a + 1) / 2;
-            if (hoff[mid] - hoff[lo] <= round_cap) a = mid; else b = mid - 1;
+    const uint32_t max_count = hc32[2];
+    if (total > 0) {
+        // Overflow rounds over point ranges whose records fit the round capacity.
+        unsigned long long round_cap = c.refine_round;
+        if (round_cap == 0) {
+            const uint64_t held_other = c.held - scratch_bytes(c, "surv_keys");
+            const uint64_t spare = c.budget > held_other + (1ull << 30) ? (c.budget - held_other - (1ull << 30)) / 8 : 0;
+            round_cap = std::max<unsigned long long>(spare, kMinRoundRecords);
         }
-        hi = std::max(a, lo + 1);
-        const unsigned long long base = hoff[lo];
-        if (hoff[hi] - base > round_cap) fail(KNNG_ERR_BUDGET, "one point's survivors exceed the round capacity");
-        cudaEvent_t r0, r1, r2;
-        KNNG_CUDA(cudaEventCreate(&r0));
-        KNNG_CUDA(cudaEventCreate(&r1));
-        KNNG_CUDA(cudaEventCreate(&r2));
-        KNNG_CUDA(cudaEventRecord(r0, c.stream));
-        if (hoff[hi] > base) {
+        round_cap = std::max<unsigned long long>(std::min<unsigned long long>(total, round_cap), max_count);
+        auto* surv =
+            static_cast<unsigned long long*>(scratch(c, "surv_keys", (round_cap + 1) * sizeof(unsigned long long)));
+        const uint32_t big_cap = pow2_at_least(std::max<uint32_t>(max_count, 2));
+        unsigned long long* big_keys = nullptr;
+        if (max_count > static_cast<uint32_t>(kApplyCap))
+            big_keys = static_cast<unsigned long long*>(scratch(
+                c, "apply_big_keys", static_cast<size_t>(148 * 2) * kRefWarps * big_cap * sizeof(unsigned long long)));
+        std::vector<unsigned long long> hoff;
+        if (total > round_cap) {
+            hoff.resize(static_cast<size_t>(n) + 1);
+            download(c, hoff.data(), soff, hoff.size());
+        }
+        uint32_t lo = 0;
+        while (lo < n) {
+            uint32_t hi = n;
+            unsigned long long base = 0;
+            if (!hoff.empty()) {
+                // Largest hi with hoff[hi] - hoff[lo] <= round_cap (at least one point).
+                uint32_t a = lo + 1, b = n;
+                while (a < b) {
+                    const uint32_t mid = a + (b - a + 1) / 2;
+                    if (hoff[mid] - hoff[lo] <= round_cap) a = mid; else b = mid - 1;
+                }
+                hi = std::max(a, lo + 1);
+                base = hoff[lo];
+                if (hoff[hi] - base > round_cap) fail(KNNG_ERR_BUDGET, "one point's survivors exceed the round capacity");
+                if (hoff[hi] == base) {
+                    lo = hi;
+                    continue;
+                }
+            }
             KNNG_CUDA(cudaMemsetAsync(sfill + lo, 0, static_cast<size_t>(hi - lo) * sizeof(uint32_t), c.stream));
             join(1, lo, hi, base, surv);
+            cudaEvent_t r1, r2;
+            KNNG_CUDA(cudaEventCreate(&r1));
+            KNNG_CUDA(cudaEventCreate(&r2));
+            KNNG_CUDA(cudaEventRecord(r1, c.stream));
+            apply(lo, hi, surv, 0, base, big_keys, big_cap);
+            KNNG_CUDA(cudaEventRecord(r2, c.stream));
+            KNNG_CUDA(cudaEventSynchronize(r2));
+            ms_apply += elapsed(r1, r2);
+            cudaEventDestroy(r1);
+            cudaEventDestroy(r2);
+            ++rec.overflow;  // rounds
+            lo = hi;
         }
-        KNNG_CUDA(cudaEventRecord(r1, c.stream));
-        KNNG_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t), c.stream));
-        const uint32_t ablocks = std::min<uint32_t>((hi - lo + kRefWarps - 1) / kRefWarps, 148 * 16);
-        k_apply<<<ablocks, kRefWarps * kWarp, 0, c.stream>>>(lo, hi, K, scount, soff, base, surv, c.set_dist,
-                                                             c.set_id, c.set_size, c.set_maxslot, c.set_bound, big,
-                                                             counters, counters + 1);
-        ++c.launches;
-        if (big_keys) {
-            k_apply_big<<<big_blocks, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, soff, base, surv,
-                                                                       big_keys, big_cap, c.set_dist, c.set_id,
-                                                                       c.set_size, c.set_maxslot, c.set_bound,
-                                                                       counters + 1);
-            ++c.launches;
-        }
-        KNNG_CUDA(cudaGetLastError());
-        KNNG_CUDA(cudaEventRecord(r2, c.stream));
-        KNNG_CUDA(cudaEventSynchronize(r2));
-        float a_ms = 0, b_ms = 0;
-        KNNG_CUDA(cudaEventElapsedTime(&a_ms, r0, r1));
-        KNNG_CUDA(cudaEventElapsedTime(&b_ms, r1, r2));
-        ms_join += a_ms;
-        ms_apply += b_ms;
-        cudaEventDestroy(r0);
-        cudaEventDestroy(r1);
-        cudaEventDestroy(r2);
-        ++rec.overflow;  // rounds
-        lo = hi;
     }
     KNNG_CUDA(cudaEventRecord(ev[2], c.stream));
     uint32_t h[2] = {0, 0};
-    unsigned long long hc[8] = {0};
+    unsigned long long hc[16] = {0};
     download(c, h, counters, 2);
-    download(c, hc, jc, 8);
+    download(c, hc, jc, 16);
     download(c, &herr, err, 1);
     if (herr) {
         for (auto& e : ev) cudaEventDestroy(e);
-        fail(KNNG_ERR_CUDA, herr == 2 ? "tensor-core join: store pass disagreed with the counting pass"
+        fail(KNNG_ERR_CUDA, herr == 2 ? "tensor-core join: overflow pass disagreed with the direct pass"
                                       : "tensor-core join: an MMA completion wait timed out");
     }
     uint64_t changed = h[1];
     KNNG_CUDA(cudaEventRecord(ev[3], c.stream));
     KNNG_CUDA(cudaEventSynchronize(ev[3]));
-    float ms_count = 0;
-    KNNG_CUDA(cudaEventElapsedTime(&ms_count, ev[0], ev[1]));
+    const float ms_all = elapsed(ev[0], ev[3]);
     for (auto& e : ev) cudaEventDestroy(e);
     rec.ms_join = ms_join_kernels;
-    rec.ms_prep = ms_count + ms_join - ms_join_kernels;
     rec.ms_apply = ms_apply;
-    rec.ms_fallback = 0;
+    rec.ms_prep = std::max(0.f, ms_all - ms_join_kernels - ms_ovf_kernels - ms_apply);
+    rec.ms_fallback = ms_ovf_kernels;
     rec.pairs = hc[0];
     rec.filter_pass = hc[1];
     rec.member_skip = hc[2];

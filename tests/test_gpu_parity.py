@@ -5,6 +5,8 @@ Bar: bit-exact index permutations, set states (distance bits, ids, sizes,
 max slots, bounds) and final ids, given the same hyperplanes and buckets."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -224,25 +226,53 @@ def test_tensor_core_tile_against_fp64(ctx, d, m, n):
     assert float((err / scale).max()) < 2.0 ** -9
 
 
-def test_refine_join_equals_pointwise(knng_lib, monkeypatch):
-    """The tensor-core local join and the one-warp-per-point pass leave
-    identical sets."""
+@pytest.fixture(scope="module")
+def refine_case(knng_lib):
+    """Sets after two repetitions of a 20k-point build, and the sets after one
+    neighbour-of-neighbour pass of the one-warp-per-point kernel."""
     pts = workloads.gaussian_mixture(n=20_000, d=100, clusters=32, sigma=0.15, seed=3)
     p = default_params(reps=2, max_leaf=257, max_leaf_odd=0, lloyd_iters=2, refine=0, seed=9)
     with KnngContext(0) as a:
         a.build(pts, p)
         s0 = a.sets()
-        ch_a = a.refine()
+    os.environ["KNNG_REFINE"] = "pointwise"
+    try:
+        with KnngContext(0) as b:
+            b.load_points(pts)
+            b.reset_sets(100)
+            b.set_sets(s0)
+            changed = b.refine()
+            s1 = b.sets()
+    finally:
+        del os.environ["KNNG_REFINE"]
+    return pts, s0, changed, s1
+
+
+@pytest.mark.parametrize("slots,round_records", [(None, None), ("0", None), ("0", "20000"), ("16", None),
+                                                 ("40", "20000")])
+def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, round_records):
+    """The tensor-core local join and the one-warp-per-point pass leave
+    identical sets, whichever way the join's survivors are stored: per-point
+    slots sized from the budget, every point through overflow rounds (one or
+    many), or small slots with the rest overflowing."""
+    pts, s0, changed, s1 = refine_case
+    if slots is not None:
+        monkeypatch.setenv("KNNG_REFINE_SLOTS", slots)
+    if round_records is not None:
+        monkeypatch.setenv("KNNG_REFINE_ROUND", round_records)
+    from sigmod23ann_b200.api import Stats
+
+    st = Stats()
+    with KnngContext(0) as a:
+        a.load_points(pts)
+        a.reset_sets(100)
+        a.set_sets(s0)
+        ch = a.refine(st)
         sa = a.sets()
-    monkeypatch.setenv("KNNG_REFINE", "pointwise")
-    with KnngContext(0) as b:
-        b.load_points(pts)
-        b.reset_sets(100)
-        b.set_sets(s0)
-        ch_b = b.refine()
-        sb = b.sets()
-    assert ch_a == ch_b
-    assert_sets_equal(sa, sb, "join vs pointwise")
+    assert ch == changed
+    assert_sets_equal(sa, s1, "join vs pointwise")
+    if round_records is not None:
+        assert st.refine_overflow > 1  # several overflow rounds
 
 
 def test_invalid_arguments(ctx):
