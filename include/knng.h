@@ -90,16 +90,17 @@ typedef struct knng_stats {
     uint64_t kernel_launches; /* all kernels launched by the call */
     uint64_t refine_changed;  /* points whose set changed in the refinement pass */
     double ms_refine_join;    /* refinement: tensor-core join, direct pass (every point) */
-    double ms_refine_apply;   /* refinement: sorted replay of survivors */
-    double ms_refine_fallback;/* refinement: join overflow rounds (points past their slots) */
+    double ms_refine_apply;   /* refinement: survivor lists + sorted replay */
+    double ms_refine_fallback;/* refinement: per-point pass for points with a lost record */
     uint64_t refine_pairs;    /* (point, candidate) pairs the join evaluated */
     uint64_t refine_filter_pass; /* pairs the tensor-core bound could not reject */
     uint64_t refine_member_skip; /* of those, candidates already in the point's list */
     uint64_t refine_exact;    /* exact FP32 distances computed by the join */
     uint64_t refine_emits;    /* survivor records written (before de-duplication) */
-    uint64_t refine_overflow; /* overflow rounds the join needed (points past their slots) */
+    uint64_t refine_overflow; /* survivor records past their point's slots (pooled) */
     double ms_refine_prep;    /* refinement: snapshot, reverse lists, scans */
-    uint64_t refine_join_launches; /* join-kernel launches of the direct pass */
+    uint64_t refine_join_launches; /* join-kernel launches */
+    uint64_t refine_lost;     /* points redone by the per-point pass (pool region full) */
 } knng_stats;
 
 /* Fills the reference's parameters: k=100, max_leaf=200, max_leaf_odd=400,

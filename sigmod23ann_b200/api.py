@@ -55,7 +55,7 @@ class Stats(Structure):
         ("ms_refine_join", c_double), ("ms_refine_apply", c_double), ("ms_refine_fallback", c_double),
         ("refine_pairs", c_uint64), ("refine_filter_pass", c_uint64), ("refine_member_skip", c_uint64),
         ("refine_exact", c_uint64), ("refine_emits", c_uint64), ("refine_overflow", c_uint64),
-        ("ms_refine_prep", c_double), ("refine_join_launches", c_uint64),
+        ("ms_refine_prep", c_double), ("refine_join_launches", c_uint64), ("refine_lost", c_uint64),
     ]
 
     def as_dict(self) -> dict:

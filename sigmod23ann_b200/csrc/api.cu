@@ -431,6 +431,7 @@ void add_refine_stats(knng_stats* stats, const Context& c, uint64_t changed, dou
     stats->refine_overflow += c.last_refine.overflow;
     stats->ms_refine_prep += c.last_refine.ms_prep;
     stats->refine_join_launches += c.last_refine.join_launches;
+    stats->refine_lost += c.last_refine.lost;
 }
 
 void validate_params(const knng_params* p) {
@@ -538,7 +539,7 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     c->device = device;
     if (const char* r = std::getenv("KNNG_REFINE")) c->refine_mode = std::strcmp(r, "pointwise") == 0 ? 1 : 0;
     if (const char* r = std::getenv("KNNG_REFINE_SLOTS")) c->refine_slots = std::max(0, std::atoi(r));
-    if (const char* r = std::getenv("KNNG_REFINE_ROUND")) c->refine_round = std::strtoull(r, nullptr, 10);
+    if (const char* r = std::getenv("KNNG_REFINE_POOL")) c->refine_pool = std::max<long long>(0, std::atoll(r));
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;

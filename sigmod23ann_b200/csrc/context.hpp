@@ -67,17 +67,16 @@ struct Context {
     // Neighbour-of-neighbour pass: 0 = local join on the tensor cores,
     // 1 = one warp per point (environment KNNG_REFINE=pointwise at creation).
     int refine_mode = 0;
-    // Survivor slots per point in the join's direct pass: -1 = sized from the
-    // free budget (environment KNNG_REFINE_SLOTS at creation overrides it,
-    // 0 = every point through the overflow rounds).
+    // Survivor storage of the join (environment at creation overrides the
+    // sizes taken from the free budget): KNNG_REFINE_SLOTS = slots per point,
+    // KNNG_REFINE_POOL = pool records per CTA region; -1 = from the budget.
     int refine_slots = -1;
-    // Records per overflow round: 0 = sized from the free budget (environment
-    // KNNG_REFINE_ROUND at creation overrides it).
-    uint64_t refine_round = 0;
+    int64_t refine_pool = -1;
     // Breakdown of the last refinement pass.
     struct RefineRecord {
         double ms_join = 0, ms_apply = 0, ms_fallback = 0, ms_prep = 0;
         uint64_t pairs = 0, filter_pass = 0, member_skip = 0, exact = 0, emits = 0, overflow = 0, join_launches = 0;
+        uint64_t lost = 0;
     } last_refine;
 };
 

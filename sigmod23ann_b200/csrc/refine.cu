@@ -387,17 +387,18 @@ __device__ __forceinline__ void stage_rows(float* __restrict__ dst, const uint32
 }
 
 
-// mode 0 (direct): counts every point's survivors exactly into surv_count and
-// writes the first `slots` of them at surv[p * slots + cursor].
-// mode 1 (overflow): for points p in [p_lo, p_hi) with surv_count[p] > slots,
-// writes all survivors at surv[surv_off[p] - base + cursor].
+// Counts every point's survivors exactly into surv_count. A point's first
+// `slots` survivors go to surv[p * slots + cursor]; the rest to this CTA's
+// pool region pool[blockIdx.x * pool_cap ...] as (p, candidate, distance
+// bits, 0). When the region is full the record is dropped and lost[p] set;
+// the CTA's final pool fill is written to pool_fill[blockIdx.x].
 template <int D>
 __global__ void __launch_bounds__(kJoinThreads, 2)
     k_join(const uint32_t* __restrict__ snap, const unsigned long long* __restrict__ rev_off,
            const uint32_t* __restrict__ rev, const float* __restrict__ pts, int ld, const float* __restrict__ bound,
-           const uint32_t* __restrict__ set_size, int K, uint32_t n, int mode, uint32_t slots, uint32_t p_lo,
-           uint32_t p_hi, uint32_t* __restrict__ surv_count, const unsigned long long* __restrict__ surv_off,
-           unsigned long long surv_base, uint32_t* __restrict__ surv_fill, unsigned long long* __restrict__ surv,
+           const uint32_t* __restrict__ set_size, int K, uint32_t n, uint32_t slots,
+           uint32_t* __restrict__ surv_count, unsigned long long* __restrict__ surv, uint4* __restrict__ pool,
+           uint32_t pool_cap, uint32_t* __restrict__ pool_fill, uint8_t* __restrict__ lost,
            uint32_t* __restrict__ error_flag, unsigned long long* __restrict__ counters) {
     using L = JoinLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -413,9 +414,11 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     __shared__ uint32_t tmem_slot;
     __shared__ uint32_t ncols_s;
     __shared__ uint32_t fullrow[kTile];
+    __shared__ uint32_t pool_cursor;
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
     if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
     if (tid == 0) {
+        pool_cursor = 0;
         tc::mbar_init(&mbar, 1);
         tc::fence_barrier_init();
     }
@@ -468,7 +471,6 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
             bool any = false;
             if (tid < kTile) {
                 uint32_t p = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
-                if (p != kNone && (p < p_lo || p >= p_hi || (mode == 1 && surv_count[p] <= slots))) p = kNone;
                 pid[tid] = p;
                 bnd[tid] = p != kNone ? bound[p] : 0.0f;
                 // A set that is not full lists its empty slots as id 0.
@@ -641,19 +643,17 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                     const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(Bo + j * D), prow);
                     if (d < bp) {
                         ++n_emit;
-                        const unsigned long long rec =
-                            (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
-                        if (mode == 0) {
-                            const uint32_t s = atomicAdd(&surv_count[p], 1u);
-                            if (s < slots) surv[static_cast<size_t>(p) * slots + s] = rec;
+                        const uint32_t s = atomicAdd(&surv_count[p], 1u);
+                        if (s < slots) {
+                            surv[static_cast<size_t>(p) * slots + s] =
+                                (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
                         } else {
-                            const uint32_t s2 = atomicAdd(&surv_fill[p], 1u);
-                            // The overflow pass repeats the direct pass exactly; the
-                            // guard keeps a disagreement from writing past p's range.
-                            if (s2 < surv_count[p])
-                                surv[surv_off[p] - surv_base + s2] = rec;
+                            const uint32_t e = atomicAdd(&pool_cursor, 1u);
+                            if (e < pool_cap)
+                                pool[static_cast<size_t>(blockIdx.x) * pool_cap + e] =
+                                    make_uint4(p, c, __float_as_uint(d), 0u);
                             else
-                                atomicExch(error_flag, 2u);
+                                lost[p] = 1;
                         }
                     }
                 }
@@ -672,6 +672,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     atomicAdd(&counters[3], n_exact);
     atomicAdd(&counters[4], n_emit);
     __syncthreads();
+    if (tid == 0) pool_fill[blockIdx.x] = min(pool_cursor, pool_cap);
     if (warp == 0) {
         tc::fence_after_sync();
         tc::tmem_dealloc(tmem, kTile);
@@ -705,33 +706,39 @@ __device__ __forceinline__ uint32_t replay_sorted(unsigned long long* buf, uint3
 
 constexpr int kApplyCap = 1024;  // survivors sorted in shared memory per warp
 
-// Points in [p_lo, p_hi). With stride > 0 (direct slots): points with at
-// most `stride` survivors, read at surv[p * stride ...]. With stride == 0
-// (overflow rounds): points with more than `skip_upto` survivors, read at
-// surv[surv_off[p] - base ...]. Lists are sorted in shared memory when they
-// fit; larger lists are queued on `big`.
+// Loads point p's S survivors into buf[0 .. P2): the first min(S, slots)
+// from its slots, the rest from its list ovf[ovf_off[p] ...]; padding ~0.
+__device__ __forceinline__ void gather_survivors(unsigned long long* buf, uint32_t S, uint32_t P2, uint32_t p,
+                                                 uint32_t slots, const unsigned long long* __restrict__ surv,
+                                                 const unsigned long long* __restrict__ ovf_off,
+                                                 const unsigned long long* __restrict__ ovf, int lane) {
+    const unsigned long long* direct = surv + static_cast<size_t>(p) * slots;
+    const unsigned long long* rest = S > slots ? ovf + ovf_off[p] : nullptr;
+    for (uint32_t t = lane; t < P2; t += kWarp)
+        buf[t] = t < S ? (t < slots ? direct[t] : rest[t - slots]) : ~0ull;
+}
+
+// Every point with survivors and no lost record: gathered, sorted in shared
+// memory when they fit, replayed; larger lists are queued on `big`.
 __global__ void __launch_bounds__(kRefWarps * kWarp)
-    k_apply(uint32_t p_lo, uint32_t p_hi, int K, const uint32_t* __restrict__ surv_count,
-            const unsigned long long* __restrict__ surv_off, unsigned long long surv_base,
-            const unsigned long long* __restrict__ surv, uint32_t stride, uint32_t skip_upto,
+    k_apply(uint32_t n, int K, const uint32_t* __restrict__ surv_count, uint32_t slots,
+            const unsigned long long* __restrict__ surv, const unsigned long long* __restrict__ ovf_off,
+            const unsigned long long* __restrict__ ovf, const uint8_t* __restrict__ lost,
             float* __restrict__ set_dist, uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size,
             uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound, uint32_t* __restrict__ big,
             uint32_t* __restrict__ big_n, uint32_t* __restrict__ changed_count) {
     __shared__ unsigned long long keys_s[kRefWarps][kApplyCap];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     unsigned long long* buf = keys_s[warp];
-    for (uint32_t p = p_lo + blockIdx.x * kRefWarps + warp; p < p_hi; p += gridDim.x * kRefWarps) {
+    for (uint32_t p = blockIdx.x * kRefWarps + warp; p < n; p += gridDim.x * kRefWarps) {
         const uint32_t S = surv_count[p];
-        if (S == 0) continue;
-        if (stride ? S > stride : S <= skip_upto) continue;
+        if (S == 0 || lost[p]) continue;
         if (S > kApplyCap) {
             if (lane == 0) big[atomicAdd(big_n, 1u)] = p;
             continue;
         }
         const uint32_t P2 = pow2_at_least(S);
-        const unsigned long long* src =
-            stride ? surv + static_cast<size_t>(p) * stride : surv + (surv_off[p] - surv_base);
-        for (uint32_t t = lane; t < P2; t += kWarp) buf[t] = t < S ? src[t] : ~0ull;
+        gather_survivors(buf, S, P2, p, slots, surv, ovf_off, ovf, lane);
         const uint32_t ch = replay_sorted(buf, S, P2, p, K, set_dist, set_id, set_size, set_maxslot, set_bound, lane);
         if (ch && lane == 0) atomicAdd(changed_count, 1u);
     }
@@ -741,8 +748,8 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
 // global scratch region of `cap` (a power of two >= the largest list) entries.
 __global__ void __launch_bounds__(kRefWarps * kWarp)
     k_apply_big(const uint32_t* __restrict__ big, const uint32_t* __restrict__ big_n, int K,
-                const uint32_t* __restrict__ surv_count, const unsigned long long* __restrict__ surv_off,
-                unsigned long long surv_base, const unsigned long long* __restrict__ surv,
+                const uint32_t* __restrict__ surv_count, uint32_t slots, const unsigned long long* __restrict__ surv,
+                const unsigned long long* __restrict__ ovf_off, const unsigned long long* __restrict__ ovf,
                 unsigned long long* __restrict__ scratch_keys, uint32_t cap, float* __restrict__ set_dist,
                 uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
                 float* __restrict__ set_bound, uint32_t* __restrict__ changed_count) {
@@ -754,8 +761,7 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
         const uint32_t p = big[w];
         const uint32_t S = surv_count[p];
         const uint32_t P2 = pow2_at_least(S);
-        const unsigned long long* src = surv + (surv_off[p] - surv_base);
-        for (uint32_t t = lane; t < P2; t += kWarp) buf[t] = t < S ? src[t] : ~0ull;
+        gather_survivors(buf, S, P2, p, slots, surv, ovf_off, ovf, lane);
         const uint32_t ch = replay_sorted(buf, S, P2, p, K, set_dist, set_id, set_size, set_maxslot, set_bound, lane);
         if (ch && lane == 0) atomicAdd(changed_count, 1u);
     }
@@ -832,22 +838,51 @@ void device_scan(Context& c, const uint32_t* in, uint64_t n, unsigned long long*
     KNNG_CUDA(cudaGetLastError());
 }
 
-// Points with more survivors than their direct slots are stored in rounds of
-// at least this many records (8 bytes each), more when the budget allows.
-constexpr uint64_t kMinRoundRecords = 1ull << 24;
-
-// ocount[p] = count[p] when it exceeds `slots`, else 0; *max_count = the
-// largest count.
-__global__ void k_overflow_counts(const uint32_t* __restrict__ count, uint32_t n, uint32_t slots,
-                                  uint32_t* __restrict__ ocount, uint32_t* __restrict__ max_count) {
+// ocount[p] = count[p] - slots for points past their slots with no lost
+// record, else 0; points with a lost record are listed (in no particular
+// order) in lost_list[0 .. *lost_n); *max_count = the largest count among
+// the others.
+__global__ void k_excess_counts(const uint32_t* __restrict__ count, const uint8_t* __restrict__ lost, uint32_t n,
+                                uint32_t slots, uint32_t* __restrict__ ocount, uint32_t* __restrict__ lost_list,
+                                uint32_t* __restrict__ lost_n, uint32_t* __restrict__ max_count) {
     uint32_t m = 0;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        const uint32_t v = count[p];
-        ocount[p] = v > slots ? v : 0u;
-        m = max(m, v);
+    const uint32_t lane = threadIdx.x % kWarp;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t p0 = blockIdx.x * blockDim.x; p0 < n; p0 += stride) {
+        const uint32_t p = p0 + threadIdx.x;
+        const uint32_t v = p < n ? count[p] : 0u;
+        const bool is_lost = p < n && lost[p] != 0;
+        if (p < n) ocount[p] = !is_lost && v > slots ? v - slots : 0u;
+        if (!is_lost) m = max(m, v);
+        const unsigned b = __ballot_sync(kFull, is_lost);
+        if (b) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(lost_n, static_cast<uint32_t>(__popc(b)));
+            base = __shfl_sync(kFull, base, 0);
+            if (is_lost) lost_list[base + __popc(b & ((1u << lane) - 1u))] = p;
+        }
     }
     for (int o = kWarp / 2; o > 0; o /= 2) m = max(m, __shfl_xor_sync(kFull, m, o));
-    if ((threadIdx.x % kWarp) == 0 && m) atomicMax(max_count, m);
+    if (lane == 0 && m) atomicMax(max_count, m);
+}
+
+// Counting-sort scatter of the pool regions into per-point lists:
+// ovf[ovf_off[p] + cursor] = (candidate << 32) | distance bits, for records
+// of points without a lost record. One block per region.
+__global__ void __launch_bounds__(256) k_pool_scatter(const uint4* __restrict__ pool, uint32_t pool_cap,
+                                                      const uint32_t* __restrict__ pool_fill,
+                                                      const uint8_t* __restrict__ lost,
+                                                      const unsigned long long* __restrict__ ovf_off,
+                                                      uint32_t* __restrict__ ovf_fill,
+                                                      unsigned long long* __restrict__ ovf) {
+    const uint32_t fill = pool_fill[blockIdx.x];
+    const uint4* region = pool + static_cast<size_t>(blockIdx.x) * pool_cap;
+    for (uint32_t i = threadIdx.x; i < fill; i += blockDim.x) {
+        const uint4 r = region[i];
+        if (lost[r.x]) continue;
+        const uint32_t at = atomicAdd(&ovf_fill[r.x], 1u);
+        ovf[ovf_off[r.x] + at] = (static_cast<unsigned long long>(r.y) << 32) | r.z;
+    }
 }
 
 }  // namespace
@@ -918,94 +953,73 @@ uint64_t run_refine(Context& c) {
     c.launches += 2;
     KNNG_CUDA(cudaGetLastError());
 
-    // Join, direct pass: exact survivor counts, and the survivors of every point
-    // with at most `slots` of them in fixed per-point slots.
-    auto* scount = static_cast<uint32_t*>(scratch(c, "surv_count", static_cast<size_t>(n) * sizeof(uint32_t)));
-    auto* ocount = static_cast<uint32_t*>(scratch(c, "surv_ovf_count", static_cast<size_t>(n) * sizeof(uint32_t)));
-    auto* sfill = static_cast<uint32_t*>(scratch(c, "surv_fill", static_cast<size_t>(n) * sizeof(uint32_t)));
-    auto* soff = static_cast<unsigned long long*>(
-        scratch(c, "surv_offsets", (static_cast<size_t>(n) + 1) * sizeof(unsigned long long)));
-    auto* err = static_cast<uint32_t*>(scratch(c, "join_error", sizeof(uint32_t)));
-    auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 16 * sizeof(unsigned long long)));
-    auto* counters = static_cast<uint32_t*>(scratch(c, "apply_counters", 4 * sizeof(uint32_t)));
-    auto* big = static_cast<uint32_t*>(scratch(c, "apply_big", static_cast<size_t>(n) * sizeof(uint32_t)));
-    KNNG_CUDA(cudaMemsetAsync(scount, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
-    KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
-    KNNG_CUDA(cudaMemsetAsync(jc, 0, 16 * sizeof(unsigned long long), c.stream));
-    KNNG_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), c.stream));
+    // Survivor storage: `slots` per point, then per-CTA pool regions for the
+    // rest, both sized from the free budget (counting what they already hold).
+    constexpr uint32_t kJoinBlocks = 148 * 2;
+    const uint64_t held_other = c.held - scratch_bytes(c, "surv_direct") - scratch_bytes(c, "surv_pool");
+    const uint64_t reserve = (1ull << 30) + static_cast<uint64_t>(n) * 32;
+    const uint64_t avail = c.budget > held_other + reserve ? c.budget - held_other - reserve : 0;
     uint32_t slots = 0;
     if (c.refine_slots >= 0) {
         slots = std::min<uint32_t>(static_cast<uint32_t>(c.refine_slots), kApplyCap);
     } else {
-        // Half of what the budget leaves free (counting the slots already held),
-        // after a reserve for the overflow rounds.
-        const uint64_t held_other = c.held - scratch_bytes(c, "surv_direct");
-        const uint64_t reserve = (1ull << 30) + kMinRoundRecords * 8;
-        const uint64_t avail = c.budget > held_other + reserve ? (c.budget - held_other - reserve) / 2 : 0;
-        slots = static_cast<uint32_t>(std::min<uint64_t>(kApplyCap, avail / (static_cast<uint64_t>(n) * 8)));
+        slots = static_cast<uint32_t>(std::min<uint64_t>(kApplyCap, avail * 2 / 5 / (static_cast<uint64_t>(n) * 8)));
         if (slots < 8) slots = 0;
     }
+    uint32_t pool_cap = 0;  // records per CTA region
+    if (c.refine_pool >= 0) {
+        pool_cap = static_cast<uint32_t>(c.refine_pool);
+    } else {
+        const uint64_t after = avail > static_cast<uint64_t>(n) * slots * 8 ? avail - static_cast<uint64_t>(n) * slots * 8 : 0;
+        pool_cap = static_cast<uint32_t>(std::min<uint64_t>(after / 2 / (kJoinBlocks * 16ull), 1u << 30));
+    }
+    auto* scount = static_cast<uint32_t*>(scratch(c, "surv_count", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* ocount = static_cast<uint32_t*>(scratch(c, "surv_excess", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* ofill = static_cast<uint32_t*>(scratch(c, "surv_excess_fill", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* lost = static_cast<uint8_t*>(scratch(c, "surv_lost", n));
+    auto* lost_list = static_cast<uint32_t*>(scratch(c, "surv_lost_list", static_cast<size_t>(n) * sizeof(uint32_t)));
+    auto* soff = static_cast<unsigned long long*>(
+        scratch(c, "surv_offsets", (static_cast<size_t>(n) + 1) * sizeof(unsigned long long)));
+    auto* pool_fill = static_cast<uint32_t*>(scratch(c, "surv_pool_fill", kJoinBlocks * sizeof(uint32_t)));
+    auto* err = static_cast<uint32_t*>(scratch(c, "join_error", sizeof(uint32_t)));
+    auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 8 * sizeof(unsigned long long)));
+    auto* counters = static_cast<uint32_t*>(scratch(c, "apply_counters", 4 * sizeof(uint32_t)));
+    auto* big = static_cast<uint32_t*>(scratch(c, "apply_big", static_cast<size_t>(n) * sizeof(uint32_t)));
     unsigned long long* direct =
         slots ? static_cast<unsigned long long*>(
                     scratch(c, "surv_direct", static_cast<size_t>(n) * slots * sizeof(unsigned long long)))
               : nullptr;
-    float ms_join_kernels = 0.f, ms_ovf_kernels = 0.f;
-    auto join = [&](int mode, uint32_t lo, uint32_t hi, unsigned long long base, unsigned long long* out) {
-        cudaEvent_t j0, j1;
-        KNNG_CUDA(cudaEventCreate(&j0));
-        KNNG_CUDA(cudaEventCreate(&j1));
-        KNNG_CUDA(cudaEventRecord(j0, c.stream));
-        KNNG_DISPATCH_D(c.d, {
-            const size_t smem = JoinLayout<D>::bytes;  // (constexpr)
-            auto kern = k_join<D>;
-            KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-            kern<<<148 * 2, kJoinThreads, smem, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K, n,
-                                                        mode, slots, lo, hi, scount, soff, base, sfill, out, err,
-                                                        mode == 0 ? jc : jc + 8);
-        });
-        ++c.launches;
-        if (mode == 0) ++rec.join_launches;
-        KNNG_CUDA(cudaGetLastError());
-        KNNG_CUDA(cudaEventRecord(j1, c.stream));
-        KNNG_CUDA(cudaEventSynchronize(j1));
-        float ms = 0.f;
-        KNNG_CUDA(cudaEventElapsedTime(&ms, j0, j1));
-        (mode == 0 ? ms_join_kernels : ms_ovf_kernels) += ms;
-        cudaEventDestroy(j0);
-        cudaEventDestroy(j1);
-    };
-    auto apply = [&](uint32_t lo, uint32_t hi, const unsigned long long* src, uint32_t stride, unsigned long long base,
-                     unsigned long long* big_keys, uint32_t big_cap) {
-        KNNG_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t), c.stream));
-        const uint32_t ablocks = std::max<uint32_t>(1, std::min<uint32_t>((hi - lo + kRefWarps - 1) / kRefWarps, 148 * 16));
-        k_apply<<<ablocks, kRefWarps * kWarp, 0, c.stream>>>(lo, hi, K, scount, soff, base, src, stride, slots,
-                                                             c.set_dist, c.set_id, c.set_size, c.set_maxslot,
-                                                             c.set_bound, big, counters, counters + 1);
-        ++c.launches;
-        if (big_keys) {
-            k_apply_big<<<148 * 2, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, soff, base, src, big_keys,
-                                                                    big_cap, c.set_dist, c.set_id, c.set_size,
-                                                                    c.set_maxslot, c.set_bound, counters + 1);
-            ++c.launches;
-        }
-        KNNG_CUDA(cudaGetLastError());
-    };
+    uint4* pool = pool_cap ? static_cast<uint4*>(
+                                 scratch(c, "surv_pool", static_cast<size_t>(kJoinBlocks) * pool_cap * sizeof(uint4)))
+                           : nullptr;
+    KNNG_CUDA(cudaMemsetAsync(scount, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(ofill, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(lost, 0, n, c.stream));
+    KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(jc, 0, 8 * sizeof(unsigned long long), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), c.stream));
     auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
         float ms = 0.f;
         KNNG_CUDA(cudaEventElapsedTime(&ms, a, b));
         return ms;
     };
     KNNG_CUDA(cudaEventRecord(ev[1], c.stream));
-    join(0, 0, n, 0, direct);
-    cudaEvent_t a0, a1;
-    KNNG_CUDA(cudaEventCreate(&a0));
-    KNNG_CUDA(cudaEventCreate(&a1));
-    KNNG_CUDA(cudaEventRecord(a0, c.stream));
-    if (slots) apply(0, n, direct, slots, 0, nullptr, 0);
-    KNNG_CUDA(cudaEventRecord(a1, c.stream));
-    // Points whose survivors overflowed their slots: CSR offsets over them alone.
+    KNNG_DISPATCH_D(c.d, {
+        const size_t smem = JoinLayout<D>::bytes;  // (constexpr)
+        auto kern = k_join<D>;
+        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        kern<<<kJoinBlocks, kJoinThreads, smem, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K,
+                                                            n, slots, scount, direct, pool, pool_cap, pool_fill, lost,
+                                                            err, jc);
+    });
+    ++c.launches;
+    ++rec.join_launches;
+    KNNG_CUDA(cudaGetLastError());
+    KNNG_CUDA(cudaEventRecord(ev[2], c.stream));
+    // Per-point lists of the pooled records, then one replay over every point.
     const uint32_t oblocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 255) / 256, 148 * 8));
-    k_overflow_counts<<<oblocks, 256, 0, c.stream>>>(scount, n, slots, ocount, counters + 2);
+    k_excess_counts<<<oblocks, 256, 0, c.stream>>>(scount, lost, n, slots, ocount, lost_list, counters + 3,
+                                                   counters + 2);
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     device_scan(c, ocount, n, soff);
@@ -1015,95 +1029,71 @@ uint64_t run_refine(Context& c) {
     download(c, hc32, counters, 4);
     uint32_t herr = 0;
     download(c, &herr, err, 1);
-    float ms_apply = elapsed(a0, a1);
-    cudaEventDestroy(a0);
-    cudaEventDestroy(a1);
     if (herr) {
         for (auto& e : ev) cudaEventDestroy(e);
         fail(KNNG_ERR_CUDA, "tensor-core join: an MMA completion wait timed out");
     }
-    const uint32_t max_count = hc32[2];
+    const uint32_t max_count = hc32[2], lost_points = hc32[3];
+    auto* ovf = static_cast<unsigned long long*>(
+        scratch(c, "surv_lists", (std::max<unsigned long long>(total, 1)) * sizeof(unsigned long long)));
     if (total > 0) {
-        // Overflow rounds over point ranges whose records fit the round capacity.
-        unsigned long long round_cap = c.refine_round;
-        if (round_cap == 0) {
-            const uint64_t held_other = c.held - scratch_bytes(c, "surv_keys");
-            const uint64_t spare = c.budget > held_other + (1ull << 30) ? (c.budget - held_other - (1ull << 30)) / 8 : 0;
-            round_cap = std::max<unsigned long long>(spare, kMinRoundRecords);
-        }
-        round_cap = std::max<unsigned long long>(std::min<unsigned long long>(total, round_cap), max_count);
-        auto* surv =
-            static_cast<unsigned long long*>(scratch(c, "surv_keys", (round_cap + 1) * sizeof(unsigned long long)));
-        const uint32_t big_cap = pow2_at_least(std::max<uint32_t>(max_count, 2));
-        unsigned long long* big_keys = nullptr;
-        if (max_count > static_cast<uint32_t>(kApplyCap))
-            big_keys = static_cast<unsigned long long*>(scratch(
-                c, "apply_big_keys", static_cast<size_t>(148 * 2) * kRefWarps * big_cap * sizeof(unsigned long long)));
-        std::vector<unsigned long long> hoff;
-        if (total > round_cap) {
-            hoff.resize(static_cast<size_t>(n) + 1);
-            download(c, hoff.data(), soff, hoff.size());
-        }
-        uint32_t lo = 0;
-        while (lo < n) {
-            uint32_t hi = n;
-            unsigned long long base = 0;
-            if (!hoff.empty()) {
-                // Largest hi with hoff[hi] - hoff[lo] <= round_cap (at least one point).
-                uint32_t a = lo + 1, b = n;
-                while (a < b) {
-                    const uint32_t mid = a + (b - a + 1) / 2;
-                    if (hoff[mid] - hoff[lo] <= round_cap) a = mid; else b = mid - 1;
-                }
-                hi = std::max(a, lo + 1);
-                base = hoff[lo];
-                if (hoff[hi] - base > round_cap) fail(KNNG_ERR_BUDGET, "one point's survivors exceed the round capacity");
-                if (hoff[hi] == base) {
-                    lo = hi;
-                    continue;
-                }
-            }
-            KNNG_CUDA(cudaMemsetAsync(sfill + lo, 0, static_cast<size_t>(hi - lo) * sizeof(uint32_t), c.stream));
-            join(1, lo, hi, base, surv);
-            cudaEvent_t r1, r2;
-            KNNG_CUDA(cudaEventCreate(&r1));
-            KNNG_CUDA(cudaEventCreate(&r2));
-            KNNG_CUDA(cudaEventRecord(r1, c.stream));
-            apply(lo, hi, surv, 0, base, big_keys, big_cap);
-            KNNG_CUDA(cudaEventRecord(r2, c.stream));
-            KNNG_CUDA(cudaEventSynchronize(r2));
-            ms_apply += elapsed(r1, r2);
-            cudaEventDestroy(r1);
-            cudaEventDestroy(r2);
-            ++rec.overflow;  // rounds
-            lo = hi;
-        }
+        k_pool_scatter<<<kJoinBlocks, 256, 0, c.stream>>>(pool, pool_cap, pool_fill, lost, soff, ofill, ovf);
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
     }
-    KNNG_CUDA(cudaEventRecord(ev[2], c.stream));
-    uint32_t h[2] = {0, 0};
-    unsigned long long hc[16] = {0};
-    download(c, h, counters, 2);
-    download(c, hc, jc, 16);
-    download(c, &herr, err, 1);
-    if (herr) {
-        for (auto& e : ev) cudaEventDestroy(e);
-        fail(KNNG_ERR_CUDA, herr == 2 ? "tensor-core join: overflow pass disagreed with the direct pass"
-                                      : "tensor-core join: an MMA completion wait timed out");
+    const uint32_t big_cap = pow2_at_least(std::max<uint32_t>(max_count, 2));
+    const uint32_t ablocks = std::max<uint32_t>(1, std::min<uint32_t>((n + kRefWarps - 1) / kRefWarps, 148 * 16));
+    k_apply<<<ablocks, kRefWarps * kWarp, 0, c.stream>>>(n, K, scount, slots, direct, soff, ovf, lost, c.set_dist,
+                                                         c.set_id, c.set_size, c.set_maxslot, c.set_bound, big,
+                                                         counters, counters + 1);
+    ++c.launches;
+    KNNG_CUDA(cudaGetLastError());
+    if (max_count > static_cast<uint32_t>(kApplyCap)) {
+        auto* big_keys = static_cast<unsigned long long*>(scratch(
+            c, "apply_big_keys", static_cast<size_t>(kJoinBlocks) * kRefWarps * big_cap * sizeof(unsigned long long)));
+        k_apply_big<<<kJoinBlocks, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, slots, direct, soff, ovf,
+                                                                    big_keys, big_cap, c.set_dist, c.set_id,
+                                                                    c.set_size, c.set_maxslot, c.set_bound,
+                                                                    counters + 1);
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
     }
-    uint64_t changed = h[1];
     KNNG_CUDA(cudaEventRecord(ev[3], c.stream));
+    // Points with a lost record (their pool region filled up): the
+    // one-warp-per-point pass over their list.
+    uint64_t changed_lost = 0;
+    float ms_lost = 0.f;
+    if (lost_points > 0) {
+        cudaEvent_t r1, r2;
+        KNNG_CUDA(cudaEventCreate(&r1));
+        KNNG_CUDA(cudaEventCreate(&r2));
+        KNNG_CUDA(cudaEventRecord(r1, c.stream));
+        changed_lost = run_refine_pointwise(c, snap, lost_list, lost_points);
+        KNNG_CUDA(cudaEventRecord(r2, c.stream));
+        KNNG_CUDA(cudaEventSynchronize(r2));
+        ms_lost = elapsed(r1, r2);
+        cudaEventDestroy(r1);
+        cudaEventDestroy(r2);
+    }
+    uint32_t h[2] = {0, 0};
+    unsigned long long hc[8] = {0};
+    download(c, h, counters, 2);
+    download(c, hc, jc, 8);
+    uint64_t changed = h[1] + changed_lost;
     KNNG_CUDA(cudaEventSynchronize(ev[3]));
     const float ms_all = elapsed(ev[0], ev[3]);
+    rec.ms_join = elapsed(ev[1], ev[2]);
+    rec.ms_apply = elapsed(ev[2], ev[3]);
+    rec.ms_prep = std::max(0.0, ms_all - rec.ms_join - rec.ms_apply);
+    rec.ms_fallback = ms_lost;
     for (auto& e : ev) cudaEventDestroy(e);
-    rec.ms_join = ms_join_kernels;
-    rec.ms_apply = ms_apply;
-    rec.ms_prep = std::max(0.f, ms_all - ms_join_kernels - ms_ovf_kernels - ms_apply);
-    rec.ms_fallback = ms_ovf_kernels;
     rec.pairs = hc[0];
     rec.filter_pass = hc[1];
     rec.member_skip = hc[2];
     rec.exact = hc[3];
     rec.emits = hc[4];
+    rec.overflow = total;
+    rec.lost = lost_points;
     c.last_refine = rec;
     return changed;
 }

@@ -45,9 +45,9 @@ def test_status_strings(knng_lib):
 
 
 def test_struct_layouts_match_header():
-    # knng_params: 8 x uint32 + uint64; knng_stats: 10 doubles + 18 uint64.
+    # knng_params: 8 x uint32 + uint64; knng_stats: 10 doubles + 19 uint64.
     assert ctypes.sizeof(api.Params) == 40
-    assert ctypes.sizeof(api.Stats) == 10 * 8 + 18 * 8
+    assert ctypes.sizeof(api.Stats) == 10 * 8 + 19 * 8
 
 
 def test_create_without_device_reports_no_device(knng_lib):

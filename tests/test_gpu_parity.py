@@ -248,20 +248,19 @@ def refine_case(knng_lib):
     return pts, s0, changed, s1
 
 
-@pytest.mark.parametrize("slots,round_records", [(None, None), ("0", None), ("0", "20000"), ("16", None),
-                                                 ("40", "20000")])
-def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, round_records):
+@pytest.mark.parametrize("slots,pool", [(None, None), ("16", None), ("0", None), ("16", "64"), ("0", "0")])
+def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, pool):
     """The tensor-core local join and the one-warp-per-point pass leave
-    identical sets, whichever way the join's survivors are stored: per-point
-    slots sized from the budget, every point through overflow rounds (one or
-    many), or small slots with the rest overflowing."""
+    identical sets, however the join's survivors are stored: per-point slots
+    sized from the budget, small or no slots with the rest pooled, or pool
+    regions so small that points lose records and are redone point by point."""
+    from sigmod23ann_b200.api import Stats
+
     pts, s0, changed, s1 = refine_case
     if slots is not None:
         monkeypatch.setenv("KNNG_REFINE_SLOTS", slots)
-    if round_records is not None:
-        monkeypatch.setenv("KNNG_REFINE_ROUND", round_records)
-    from sigmod23ann_b200.api import Stats
-
+    if pool is not None:
+        monkeypatch.setenv("KNNG_REFINE_POOL", pool)
     st = Stats()
     with KnngContext(0) as a:
         a.load_points(pts)
@@ -271,8 +270,10 @@ def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, round_rec
         sa = a.sets()
     assert ch == changed
     assert_sets_equal(sa, s1, "join vs pointwise")
-    if round_records is not None:
-        assert st.refine_overflow > 1  # several overflow rounds
+    if slots is not None and pool is None:
+        assert st.refine_overflow > 0 and st.refine_lost == 0  # records pooled, none lost
+    if pool is not None:
+        assert st.refine_lost > 0  # points redone point by point
 
 
 def test_invalid_arguments(ctx):
