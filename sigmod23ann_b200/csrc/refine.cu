@@ -284,77 +284,129 @@ __global__ void k_rev_fill(const uint32_t* __restrict__ snap, uint32_t n, int K,
 }
 
 constexpr int kJoinThreads = 256;
-constexpr int kTile = 128;  // MMA M = N = 128
+constexpr int kTile = 128;      // MMA M (rows of R(q) per chunk)
 
 template <int D>
 struct JoinLayout {
     static constexpr int KP = (D + 7) / 8 * 8;  // K padded to the MMA step (8 tf32)
     static constexpr int CH = KP / 4;           // 16-byte chunks per row
     static constexpr size_t tile_bytes = static_cast<size_t>(kTile) * KP * 4;
-    // A', B' (centred TF32 tiles) and per-row scalars (about 108 KB at D = 100:
-    // two CTAs per SM).  Once the MMA has consumed A' and B', their space holds
-    // p's sorted lists, then the original FP32 rows.
     static_assert(tile_bytes >= static_cast<size_t>(kTile) * D * 4, "original rows must fit in a tile");
-    static_assert(2 * tile_bytes >= static_cast<size_t>(kTile) * kMaxK * 4, "lists must fit in the two tiles");
-    static constexpr size_t bytes = 2 * tile_bytes + 5 * kTile * 4 + 128 * 4 + 16;
 };
 
+// Columns of the B tile: S(q) has at most k distinct ids; the MMA takes N in
+// steps of 16.
+__host__ __device__ constexpr uint32_t join_cols(uint32_t K) { return K <= 16 ? 16u : (K + 15) / 16 * 16; }
+
+// Dynamic shared memory of k_join (byte offsets).  A' (128 x KP) and B'
+// (NB x KP) hold the centred TF32 tiles; once the MMA has consumed them, the
+// rows' sorted lists S(p), then the original FP32 rows (row-major, D
+// floats).  `x` holds the per-thread pair masks and their prefix sums.
+struct JoinSmem {
+    uint32_t a, b, norm_a, norm_b, bnd, pid, cid, fullrow, centre, x, bytes;
+};
+
+__host__ __device__ inline JoinSmem join_smem(int D, uint32_t K) {
+    const uint32_t KP = (D + 7) / 8 * 8;
+    JoinSmem s{};
+    s.a = 0;
+    s.b = s.a + kTile * KP * 4;
+    s.norm_a = s.b + join_cols(K) * KP * 4;
+    s.norm_b = s.norm_a + kTile * 4;
+    s.bnd = s.norm_b + kTile * 4;
+    s.pid = s.bnd + kTile * 4;
+    s.cid = s.pid + kTile * 4;
+    s.fullrow = s.cid + kTile * 4;
+    s.centre = s.fullrow + kTile * 4;
+    s.x = s.centre + (static_cast<uint32_t>(D) + 3) / 4 * 16;
+    // todo (u64 per thread), prefix sums (kJoinThreads + 1), warp totals (8)
+    s.bytes = s.x + kJoinThreads * 8 + (kJoinThreads + 1) * 4 + 8 * 4;
+    return s;
+}
+
+// Row stride (in ids) of the staged sorted lists: odd, so that the threads of
+// a warp (one row each) search on distinct banks, when 128 such rows fit in
+// the tiles' space.
+__host__ __device__ inline int list_stride(int D, uint32_t K) {
+    const uint32_t KP = (D + 7) / 8 * 8;
+    const uint32_t space = (kTile + join_cols(K)) * KP * 4;
+    return static_cast<uint32_t>(kTile) * (K | 1u) * 4 <= space ? static_cast<int>(K | 1u) : static_cast<int>(K);
+}
+
 // rows[r] (r < count and ids[r] != kNone, else zeros) minus `centre`, into a
-// chunk-major tile.  Lane l of a warp handles row (8g + l % 8), chunk
-// (4h + l / 8): every global sector read is used whole and each quarter-warp's
-// 16-byte shared stores land on distinct banks.
+// chunk-major tile of `rows` rows (a multiple of 8).  Lane l of a warp
+// handles row (8g + l % 8), chunk (4h + l / 8): every global sector read is
+// used whole and each quarter-warp's 16-byte shared stores land on distinct
+// banks.
 template <int D>
-__device__ __forceinline__ void stage_centred(float* __restrict__ tile, const uint32_t* __restrict__ ids,
+__device__ __forceinline__ void stage_centred(float* __restrict__ tile, uint32_t rows, const uint32_t* __restrict__ ids,
                                               uint32_t count, const float* __restrict__ pts, int ld,
                                               const float* __restrict__ centre) {
     constexpr int CH = JoinLayout<D>::CH;
-    constexpr int CG = (CH + 3) / 4;                                   // chunk groups
-    constexpr int ITER = ((kTile / 8) * CG + kJoinThreads / kWarp - 1) / (kJoinThreads / kWarp);
+    constexpr int CG = (CH + 3) / 4;  // chunk groups
+    constexpr int WARPS = kJoinThreads / kWarp;
     constexpr int BATCH = 4;
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     const int rl = lane & 7, cl = lane >> 3;
+    const int groups = static_cast<int>(rows / 8);
+    const int tasks = groups * CG;
+    // Task w = (chunk group w / groups, row group w % groups); this warp's
+    // tasks are warp, warp + WARPS, ...: the pair is advanced, not divided.
+    int g = warp, cg = 0;
+    while (g >= groups) {
+        g -= groups;
+        ++cg;
+    }
 #pragma unroll 1
-    for (int b0 = 0; b0 < ITER; b0 += BATCH) {
-    float4 v[BATCH];
-    // A batch of loads is issued before its stores.
+    for (int t0 = warp; t0 < tasks; t0 += BATCH * WARPS) {
+        float4 v[BATCH];
+        int tr[BATCH], tch[BATCH];
 #pragma unroll
-    for (int bi = 0; bi < BATCH; ++bi) {
-        const int it = b0 + bi;
-        const int w = warp + it * (kJoinThreads / kWarp);
-        const int r = (w % (kTile / 8)) * 8 + rl;
-        const int ch = (w / (kTile / 8)) * 4 + cl;
-        v[bi] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (it < ITER && w < (kTile / 8) * CG && ch < CH && static_cast<uint32_t>(r) < count && 4 * ch < D &&
-            ids[r] != kNone)
-            v[bi] = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + ch);
-    }
-#pragma unroll
-    for (int bi = 0; bi < BATCH; ++bi) {
-        const int it = b0 + bi;
-        const int w = warp + it * (kJoinThreads / kWarp);
-        const int r = (w % (kTile / 8)) * 8 + rl;
-        const int ch = (w / (kTile / 8)) * 4 + cl;
-        if (it < ITER && w < (kTile / 8) * CG && ch < CH) {
-            float4 x = v[bi];
-            if (static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
-                const float4 m = reinterpret_cast<const float4*>(centre)[ch];
-                x = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z), __fsub_rn(x.w, m.w));
+        for (int bi = 0; bi < BATCH; ++bi) {
+            tr[bi] = g * 8 + rl;
+            tch[bi] = cg * 4 + cl;
+            g += WARPS;
+            while (g >= groups) {
+                g -= groups;
+                ++cg;
             }
-            *reinterpret_cast<float4*>(reinterpret_cast<unsigned char*>(tile) + tc::chunk_offset(r, 4 * ch, kTile)) = x;
         }
-    }
+        // A batch of loads is issued before its stores.
+#pragma unroll
+        for (int bi = 0; bi < BATCH; ++bi) {
+            const int w = t0 + bi * WARPS;
+            const int r = tr[bi], ch = tch[bi];
+            v[bi] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (w < tasks && ch < CH && static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone)
+                v[bi] = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + ch);
+        }
+#pragma unroll
+        for (int bi = 0; bi < BATCH; ++bi) {
+            const int w = t0 + bi * WARPS;
+            const int r = tr[bi], ch = tch[bi];
+            if (w < tasks && ch < CH) {
+                float4 x = v[bi];
+                if (static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
+                    const float4 m = reinterpret_cast<const float4*>(centre)[ch];
+                    x = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z),
+                                    __fsub_rn(x.w, m.w));
+                }
+                *reinterpret_cast<float4*>(reinterpret_cast<unsigned char*>(tile) + tc::chunk_offset(r, 4 * ch, rows)) =
+                    x;
+            }
+        }
     }
 }
 
 // Squared norm of row r of a chunk-major tile (any order: only feeds the bound).
 template <int D>
-__device__ __forceinline__ float tile_norm(const float* __restrict__ tile, int r) {
+__device__ __forceinline__ float tile_norm(const float* __restrict__ tile, int r, uint32_t rows) {
     constexpr int CH = JoinLayout<D>::CH;
     float s = 0.f;
 #pragma unroll 4
     for (int ch = 0; ch < CH; ++ch) {
         const float4 v = *reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(tile) +
-                                                          tc::chunk_offset(r, 4 * ch, kTile));
+                                                          tc::chunk_offset(r, 4 * ch, rows));
         s = fmaf(v.x, v.x, fmaf(v.y, v.y, fmaf(v.z, v.z, fmaf(v.w, v.w, s))));
     }
     return s;
@@ -386,12 +438,18 @@ __device__ __forceinline__ void stage_rows(float* __restrict__ dst, const uint32
     }
 }
 
-
-// Counts every point's survivors exactly into surv_count. A point's first
-// `slots` survivors go to surv[p * slots + cursor]; the rest to this CTA's
-// pool region pool[blockIdx.x * pool_cap ...] as (p, candidate, distance
-// bits, 0). When the region is full the record is dropped and lost[p] set;
-// the CTA's final pool fill is written to pool_fill[blockIdx.x].
+// The local join of one neighbour-of-neighbour pass.  For every point q: the
+// rows R(q) (points whose snapshot list holds q), in chunks of 128, against
+// the columns S(q) (q's snapshot list, distinct ids).  A tcgen05 TF32 tile of
+// centred dot products rejects the pairs that provably cannot beat bound(p);
+// members of S(p) are dropped (binary searches, four in lockstep, in S(p)
+// staged in shared memory); the remaining pairs get the exact FP32 distance,
+// spread evenly over the CTA's threads.  Every point's survivors (distance < bound(p)) are counted exactly
+// into surv_count.  A point's first `slots` survivors go to
+// surv[p * slots + cursor]; the rest to this CTA's pool region
+// pool[blockIdx.x * pool_cap ...] as (p, candidate, distance bits, 0).  When
+// the region is full the record is dropped and lost[p] set; the CTA's final
+// pool fill is written to pool_fill[blockIdx.x].
 template <int D>
 __global__ void __launch_bounds__(kJoinThreads, 2)
     k_join(const uint32_t* __restrict__ snap, const unsigned long long* __restrict__ rev_off,
@@ -402,18 +460,23 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
            uint32_t* __restrict__ error_flag, unsigned long long* __restrict__ counters) {
     using L = JoinLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
-    float* A = reinterpret_cast<float*>(smem);
-    float* B = reinterpret_cast<float*>(smem + L::tile_bytes);
-    float* normA = reinterpret_cast<float*>(smem + 2 * L::tile_bytes);
-    float* normB = normA + kTile;
-    float* bnd = normB + kTile;
-    uint32_t* pid = reinterpret_cast<uint32_t*>(bnd + kTile);
-    uint32_t* cid = pid + kTile;
-    float* centre = reinterpret_cast<float*>(cid + kTile);
+    const JoinSmem S = join_smem(D, static_cast<uint32_t>(K));
+    const uint32_t NB = join_cols(static_cast<uint32_t>(K));
+    float* A = reinterpret_cast<float*>(smem + S.a);
+    float* B = reinterpret_cast<float*>(smem + S.b);
+    float* normA = reinterpret_cast<float*>(smem + S.norm_a);
+    float* normB = reinterpret_cast<float*>(smem + S.norm_b);
+    float* bnd = reinterpret_cast<float*>(smem + S.bnd);
+    uint32_t* pid = reinterpret_cast<uint32_t*>(smem + S.pid);
+    uint32_t* cid = reinterpret_cast<uint32_t*>(smem + S.cid);
+    uint32_t* fullrow = reinterpret_cast<uint32_t*>(smem + S.fullrow);
+    float* centre = reinterpret_cast<float*>(smem + S.centre);
+    unsigned long long* todo_s = reinterpret_cast<unsigned long long*>(smem + S.x);   // [kJoinThreads]
+    uint32_t* pref = reinterpret_cast<uint32_t*>(smem + S.x + kJoinThreads * 8);      // [kJoinThreads + 1]
+    uint32_t* wsum = pref + kJoinThreads + 1;                                          // [8]
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     __shared__ uint32_t ncols_s;
-    __shared__ uint32_t fullrow[kTile];
     __shared__ uint32_t pool_cursor;
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
     if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
@@ -426,13 +489,16 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    const uint32_t idesc = tc::idesc_tf32(kTile, kTile);
+    const uint32_t idesc = tc::idesc_tf32(kTile, NB);
     uint32_t phase = 0;
     bool healthy = true;
     unsigned long long n_pairs = 0, n_pass = 0, n_member = 0, n_exact = 0, n_emit = 0;
     const int quarter = warp % 4, half = warp / 4;
     const int row = quarter * kWarp + lane;  // TMEM lane / tile row of this thread
     const unsigned lt = (1u << lane) - 1u;
+    const int KS = list_stride(D, static_cast<uint32_t>(K));
+    int search_top = 1;  // largest power of two <= K (branch-free lower bound)
+    while (search_top * 2 <= K) search_top *= 2;
     for (uint32_t q = blockIdx.x; q < n && healthy; q += gridDim.x) {
         const unsigned long long rb = rev_off[q], re = rev_off[q + 1];
         if (rb == re) continue;
@@ -463,30 +529,29 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
         for (int j = tid; j < D; j += kJoinThreads) centre[j] = pts[static_cast<size_t>(q) * ld + j];
         __syncthreads();
         const uint32_t nc = ncols_s;
-        stage_centred<D>(B, cid, nc, pts, ld, centre);
+        stage_centred<D>(B, NB, cid, nc, pts, ld, centre);
         __syncthreads();
-        if (tid < kTile) normB[tid] = tile_norm<D>(B, tid);
+        if (static_cast<uint32_t>(tid) < NB) normB[tid] = tile_norm<D>(B, tid, NB);
         for (unsigned long long cb = rb; cb < re && healthy; cb += kTile) {
             const uint32_t m = static_cast<uint32_t>(min(static_cast<unsigned long long>(kTile), re - cb));
             bool any = false;
             if (tid < kTile) {
-                uint32_t p = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
+                const uint32_t p = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
                 pid[tid] = p;
                 bnd[tid] = p != kNone ? bound[p] : 0.0f;
-                // A set that is not full lists its empty slots as id 0.
                 fullrow[tid] = p != kNone && set_size[p] == static_cast<uint32_t>(K) ? 1u : 0u;
                 any = p != kNone;
             }
             if (!__syncthreads_or(any)) continue;
-            stage_centred<D>(A, pid, m, pts, ld, centre);
+            stage_centred<D>(A, kTile, pid, m, pts, ld, centre);
             __syncthreads();
-            if (tid < kTile) normA[tid] = tile_norm<D>(A, tid);
+            if (tid < kTile) normA[tid] = tile_norm<D>(A, tid, kTile);
             tc::fence_proxy_async();
             tc::fence_before_sync();
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after_sync();
-                tc::issue_tile_tf32(tmem, tc::smem_u32(A), tc::smem_u32(B), kTile, kTile, L::KP, idesc);
+                tc::issue_tile_tf32(tmem, tc::smem_u32(A), tc::smem_u32(B), kTile, NB, L::KP, idesc);
                 tc::mma_commit(&mbar);
             }
             const bool done = tc::mbar_wait(&mbar, phase);
@@ -497,10 +562,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                 break;
             }
             tc::fence_after_sync();
-            // p's list S(p), sorted, staged into the space A' and B' occupied with
-            // an odd row stride (conflict-free binary searches by row).
-            const int KS = static_cast<size_t>(kTile) * (K | 1) * 4 <= 2 * L::tile_bytes ? (K | 1) : K;
-            const uint32_t* lists = reinterpret_cast<const uint32_t*>(A);
+            // p's list S(p), sorted, staged into the space A' and B' occupied
+            // (row stride KS).
             {
                 uint32_t* dst = reinterpret_cast<uint32_t*>(A);
                 const uint32_t total = m * static_cast<uint32_t>(K);
@@ -570,6 +633,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
 #pragma unroll 1
                 for (int cc = 0; cc < 4; ++cc) {
                     const int j0 = half * 64 + cc * 16;
+                    if (j0 >= static_cast<int>(nc)) break;  // warp-uniform
                     float g[16];
                     tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
                     tc::tmem_wait_ld();
@@ -595,65 +659,122 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                     const int valid_cols = max(0, min(16, static_cast<int>(nc) - j0));
                     pass &= valid_cols == 16 ? 0xFFFFu : ((1u << valid_cols) - 1u);
                     if (p == kNone) pass = 0;
-                    // Members of S(p) are rejected by the set update: drop them.
-                    // (A set that is not full lists its empty slots as id 0.)
-                    uint32_t keep = pass;
-                    const uint32_t* mylist = lists + row * KS;
-                    const bool full = row < static_cast<int>(m) && fullrow[row] != 0u;
-                    uint32_t scan = pass;
-                    while (scan) {
-                        const int u = __ffs(scan) - 1;
-                        scan &= scan - 1;
-                        const uint32_t c = cid[j0 + u];
-                        if (c == 0 && !full) continue;
-                        int lo = 0, hi = K;
-                        while (lo < hi) {
-                            const int mid = (lo + hi) >> 1;
-                            if (mylist[mid] < c) lo = mid + 1; else hi = mid;
-                        }
-                        if (lo < K && mylist[lo] == c) keep &= ~(1u << u);
-                    }
                     if (p != kNone) {
                         n_pairs += valid_cols;
                         n_pass += __popc(pass);
-                        n_member += __popc(pass & ~keep);
                     }
-                    todo |= static_cast<unsigned long long>(keep) << (cc * 16);
+                    todo |= static_cast<unsigned long long>(pass) << (cc * 16);
+                }
+                // Members of S(p) are rejected by the set update: drop them.
+                // Lower bounds of four candidates at a time (branch-free, in
+                // lockstep); a set that is not full lists its empty slots as
+                // id 0, which is not taken for a member.
+                const uint32_t* mylist = reinterpret_cast<const uint32_t*>(A) + row * KS;
+                const bool full = row < static_cast<int>(m) && fullrow[row] != 0u;
+                unsigned long long scan = todo;
+#pragma unroll 1
+                while (scan) {
+                    int bit[4];
+                    uint32_t key[4];
+                    int pos[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        bit[u] = -1;
+                        key[u] = 0;
+                        pos[u] = 0;
+                        if (scan) {
+                            bit[u] = __ffsll(scan) - 1;
+                            scan &= scan - 1;
+                            key[u] = cid[half * 64 + bit[u]];
+                        }
+                    }
+                    for (int step = search_top; step > 0; step >>= 1) {
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int t = pos[u] + step;
+                            if (t <= K && mylist[t - 1] < key[u]) pos[u] = t;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        if (bit[u] >= 0 && pos[u] < K && mylist[pos[u]] == key[u] && (key[u] != 0 || full)) {
+                            todo &= ~(1ull << bit[u]);
+                            ++n_member;
+                        }
+                    }
                 }
             }
             tc::fence_before_sync();
             __syncthreads();
-            // The tiles are consumed: refill their space with the original FP32
-            // rows (row-major, D floats) for the exact distances.
+            // Pair masks and their block-wide prefix sums, then the original
+            // FP32 rows in the tiles' space.
+            todo_s[tid] = todo;
+            uint32_t x = static_cast<uint32_t>(__popcll(todo));
+#pragma unroll
+            for (int o = 1; o < kWarp; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == kWarp - 1) wsum[warp] = x;
             float* Aorig = A;
             float* Bo = B;
             stage_rows<D>(Aorig, pid, m, pts, ld);
             stage_rows<D>(Bo, cid, nc, pts, ld);
             __syncthreads();
-            if (p != kNone) {
-                const float4* prow = reinterpret_cast<const float4*>(Aorig + row * D);
+            {
+                uint32_t before = 0, total = 0;
+#pragma unroll
+                for (int w = 0; w < kJoinThreads / kWarp; ++w) {
+                    const uint32_t s = wsum[w];
+                    before += w < warp ? s : 0u;
+                    total += s;
+                }
+                pref[tid] = before + x - static_cast<uint32_t>(__popcll(todo));
+                if (tid == 0) pref[kJoinThreads] = total;
+            }
+            __syncthreads();
+            // Exact distances: pair indices [tid*T/256, (tid+1)*T/256) of the
+            // block's T pairs, in owner-thread then column order.
+            const uint32_t T = pref[kJoinThreads];
+            uint32_t lo = static_cast<uint32_t>((static_cast<unsigned long long>(tid) * T) / kJoinThreads);
+            const uint32_t hi = static_cast<uint32_t>((static_cast<unsigned long long>(tid + 1) * T) / kJoinThreads);
+            if (lo < hi) {
+                // Owner: the last thread o with pref[o] <= lo.
+                int a = 0, b = kJoinThreads - 1;
+                while (a < b) {
+                    const int mid = (a + b + 1) >> 1;
+                    if (pref[mid] <= lo) a = mid; else b = mid - 1;
+                }
+                int o = a;
+                unsigned long long bits = todo_s[o];
+                for (uint32_t r = lo - pref[o]; r > 0; --r) bits &= bits - 1;
 #pragma unroll 1
-                while (todo) {
-                    const int b = __ffsll(todo) - 1;
-                    todo &= todo - 1;
-                    const int j = half * 64 + b;
+                for (; lo < hi; ++lo) {
+                    while (bits == 0) bits = todo_s[++o];
+                    const int bit = __ffsll(bits) - 1;
+                    bits &= bits - 1;
+                    const int ow = o / kWarp;
+                    const int prow = (ow % 4) * kWarp + (o % kWarp);
+                    const int j = (ow / 4) * 64 + bit;
+                    const uint32_t pp = pid[prow];
                     const uint32_t c = cid[j];
-                    if (c == p) continue;
+                    if (c == pp) continue;
                     ++n_exact;
-                    const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(Bo + j * D), prow);
-                    if (d < bp) {
+                    const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(Bo + j * D),
+                                                                reinterpret_cast<const float4*>(Aorig + prow * D));
+                    if (d < bnd[prow]) {
                         ++n_emit;
-                        const uint32_t s = atomicAdd(&surv_count[p], 1u);
+                        const uint32_t s = atomicAdd(&surv_count[pp], 1u);
                         if (s < slots) {
-                            surv[static_cast<size_t>(p) * slots + s] =
+                            surv[static_cast<size_t>(pp) * slots + s] =
                                 (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
                         } else {
                             const uint32_t e = atomicAdd(&pool_cursor, 1u);
                             if (e < pool_cap)
                                 pool[static_cast<size_t>(blockIdx.x) * pool_cap + e] =
-                                    make_uint4(p, c, __float_as_uint(d), 0u);
+                                    make_uint4(pp, c, __float_as_uint(d), 0u);
                             else
-                                lost[p] = 1;
+                                lost[pp] = 1;
                         }
                     }
                 }
@@ -661,7 +782,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
             __syncthreads();
             // The next chunk restages B' (its space now holds original rows).
             if (cb + kTile < re) {
-                stage_centred<D>(B, cid, nc, pts, ld, centre);
+                stage_centred<D>(B, NB, cid, nc, pts, ld, centre);
                 __syncthreads();
             }
         }
@@ -793,8 +914,8 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    stage_centred<D>(A, ids, m, a, D, zero);
-    stage_centred<D>(B, ids, n, b, D, zero);
+    stage_centred<D>(A, kTile, ids, m, a, D, zero);
+    stage_centred<D>(B, kTile, ids, n, b, D, zero);
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
@@ -953,9 +1074,32 @@ uint64_t run_refine(Context& c) {
     c.launches += 2;
     KNNG_CUDA(cudaGetLastError());
 
+    // Join grid: as many CTAs as fit on the SMs at once (two per SM at
+    // d = 100, k = 100); each owns one pool region.
+    const uint32_t join_bytes = join_smem(static_cast<int>(c.d), static_cast<uint32_t>(K)).bytes;
+    // CTAs per SM from the SM's shared memory and registers (the kernel's
+    // launch bounds ask for two).
+    int sms = 0, smem_sm = 0, smem_reserved = 0, regs_sm = 0;
+    KNNG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+    KNNG_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.device));
+    KNNG_CUDA(cudaDeviceGetAttribute(&smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, c.device));
+    KNNG_CUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c.device));
+    cudaFuncAttributes fa{};
+    KNNG_DISPATCH_D(c.d, {
+        auto kern = k_join<D>;
+        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(join_bytes)));
+        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       static_cast<int>(cudaSharedmemCarveoutMaxShared)));
+        KNNG_CUDA(cudaFuncGetAttributes(&fa, kern));
+    });
+    const size_t per_cta_smem = join_bytes + fa.sharedSizeBytes + static_cast<size_t>(smem_reserved);
+    const int by_smem = static_cast<int>(static_cast<size_t>(smem_sm) / per_cta_smem);
+    const int by_regs = fa.numRegs > 0 ? regs_sm / (fa.numRegs * kJoinThreads) : 2;
+    const int per_sm = std::min({by_smem, by_regs, 2});
+    if (per_sm < 1) fail(KNNG_ERR_UNSUPPORTED, "the join kernel does not fit on an SM");
+    const uint32_t kJoinBlocks = static_cast<uint32_t>(sms) * static_cast<uint32_t>(per_sm);
     // Survivor storage: `slots` per point, then per-CTA pool regions for the
     // rest, both sized from the free budget (counting what they already hold).
-    constexpr uint32_t kJoinBlocks = 148 * 2;
     const uint64_t held_other = c.held - scratch_bytes(c, "surv_direct") - scratch_bytes(c, "surv_pool");
     const uint64_t reserve = (1ull << 30) + static_cast<uint64_t>(n) * 32;
     const uint64_t avail = c.budget > held_other + reserve ? c.budget - held_other - reserve : 0;
@@ -971,7 +1115,10 @@ uint64_t run_refine(Context& c) {
         pool_cap = static_cast<uint32_t>(c.refine_pool);
     } else {
         const uint64_t after = avail > static_cast<uint64_t>(n) * slots * 8 ? avail - static_cast<uint64_t>(n) * slots * 8 : 0;
-        pool_cap = static_cast<uint32_t>(std::min<uint64_t>(after / 2 / (kJoinBlocks * 16ull), 1u << 30));
+        // At most 128 records per point on average (the records past the
+        // slots are a small fraction once the slots hold the typical list).
+        const uint64_t want = (static_cast<uint64_t>(n) * 128 + kJoinBlocks - 1) / kJoinBlocks;
+        pool_cap = static_cast<uint32_t>(std::min<uint64_t>({after / 2 / (kJoinBlocks * 16ull), want, 1u << 30}));
     }
     auto* scount = static_cast<uint32_t*>(scratch(c, "surv_count", static_cast<size_t>(n) * sizeof(uint32_t)));
     auto* ocount = static_cast<uint32_t*>(scratch(c, "surv_excess", static_cast<size_t>(n) * sizeof(uint32_t)));
@@ -1005,10 +1152,7 @@ uint64_t run_refine(Context& c) {
     };
     KNNG_CUDA(cudaEventRecord(ev[1], c.stream));
     KNNG_DISPATCH_D(c.d, {
-        const size_t smem = JoinLayout<D>::bytes;  // (constexpr)
-        auto kern = k_join<D>;
-        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        kern<<<kJoinBlocks, kJoinThreads, smem, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K,
+        k_join<D><<<kJoinBlocks, kJoinThreads, join_bytes, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K,
                                                             n, slots, scount, direct, pool, pool_cap, pool_fill, lost,
                                                             err, jc);
     });

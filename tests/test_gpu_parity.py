@@ -248,7 +248,7 @@ def refine_case(knng_lib):
     return pts, s0, changed, s1
 
 
-@pytest.mark.parametrize("slots,pool", [(None, None), ("16", None), ("0", None), ("16", "64"), ("0", "0")])
+@pytest.mark.parametrize("slots,pool", [(None, None), ("16", "1000000"), ("0", "1000000"), ("16", "64"), ("0", "0")])
 def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, pool):
     """The tensor-core local join and the one-warp-per-point pass leave
     identical sets, however the join's survivors are stored: per-point slots
@@ -270,9 +270,9 @@ def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, pool):
         sa = a.sets()
     assert ch == changed
     assert_sets_equal(sa, s1, "join vs pointwise")
-    if slots is not None and pool is None:
+    if pool is not None and int(pool) >= 1000000:
         assert st.refine_overflow > 0 and st.refine_lost == 0  # records pooled, none lost
-    if pool is not None:
+    if pool is not None and int(pool) < 1000000:
         assert st.refine_lost > 0  # points redone point by point
 
 
