@@ -319,8 +319,9 @@ __host__ __device__ inline JoinSmem join_smem(int D, uint32_t K) {
     s.fullrow = s.cid + kTile * 4;
     s.centre = s.fullrow + kTile * 4;
     s.x = s.centre + (static_cast<uint32_t>(D) + 3) / 4 * 16;
-    // todo (u64 per thread), prefix sums (kJoinThreads + 1), warp totals (8)
-    s.bytes = s.x + kJoinThreads * 8 + (kJoinThreads + 1) * 4 + 8 * 4;
+    // pair masks and member masks (u64 per thread each), prefix sums
+    // (kJoinThreads + 1), warp totals (8)
+    s.bytes = s.x + 2 * kJoinThreads * 8 + (kJoinThreads + 1) * 4 + 8 * 4;
     return s;
 }
 
@@ -332,6 +333,82 @@ __host__ __device__ inline int list_stride(int D, uint32_t K) {
     const uint32_t space = (kTile + join_cols(K)) * KP * 4;
     return static_cast<uint32_t>(kTile) * (K | 1u) * 4 <= space ? static_cast<int>(K | 1u) : static_cast<int>(K);
 }
+
+// Block-wide exclusive prefix sums of the set bits of every thread's pair
+// mask: call scan_masks_warp, __syncthreads, scan_masks_block,
+// __syncthreads; then pref[t] is the first pair index of thread t and
+// pref[kJoinThreads] the number of pairs.
+__device__ __forceinline__ uint32_t scan_masks_warp(unsigned long long mask, uint32_t* __restrict__ wsum) {
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    uint32_t x = static_cast<uint32_t>(__popcll(mask));
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == kWarp - 1) wsum[warp] = x;
+    return x;  // inclusive, within the warp
+}
+
+__device__ __forceinline__ void scan_masks_block(unsigned long long mask, uint32_t incl, const uint32_t* __restrict__ wsum,
+                                                 uint32_t* __restrict__ pref) {
+    const int warp = threadIdx.x / kWarp;
+    uint32_t before = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kJoinThreads / kWarp; ++w) {
+        const uint32_t s = wsum[w];
+        before += w < warp ? s : 0u;
+        total += s;
+    }
+    pref[threadIdx.x] = before + incl - static_cast<uint32_t>(__popcll(mask));
+    if (threadIdx.x == 0) pref[kJoinThreads] = total;
+}
+
+// This thread's share [lo, hi) of the block's pairs (an even split), and the
+// position of pair lo: owner thread o and the owner's mask with the pairs
+// before lo cleared.
+struct PairCursor {
+    uint32_t lo, hi;
+    int o;
+    unsigned long long bits;
+};
+
+__device__ __forceinline__ PairCursor pair_share(const uint32_t* __restrict__ pref,
+                                                 const unsigned long long* __restrict__ masks) {
+    PairCursor c;
+    const uint32_t T = pref[kJoinThreads];
+    c.lo = static_cast<uint32_t>((static_cast<unsigned long long>(threadIdx.x) * T) / kJoinThreads);
+    c.hi = static_cast<uint32_t>((static_cast<unsigned long long>(threadIdx.x + 1) * T) / kJoinThreads);
+    c.o = 0;
+    c.bits = 0;
+    if (c.lo < c.hi) {
+        // Owner: the last thread o with pref[o] <= lo (it has pairs left).
+        int a = 0, b = kJoinThreads - 1;
+        while (a < b) {
+            const int mid = (a + b + 1) >> 1;
+            if (pref[mid] <= c.lo) a = mid; else b = mid - 1;
+        }
+        c.o = a;
+        c.bits = masks[a];
+        for (uint32_t r = c.lo - pref[a]; r > 0; --r) c.bits &= c.bits - 1;
+    }
+    return c;
+}
+
+// Next pair of the cursor (call while lo < hi): owner thread and column bit.
+__device__ __forceinline__ void pair_next(PairCursor& c, const unsigned long long* __restrict__ masks, int& owner,
+                                          int& bit) {
+    while (c.bits == 0) c.bits = masks[++c.o];
+    owner = c.o;
+    bit = __ffsll(c.bits) - 1;
+    c.bits &= c.bits - 1;
+    ++c.lo;
+}
+
+// Tile row and column of bit `bit` of thread o's mask (thread o owns TMEM
+// lane (o / 32 % 4) * 32 + o % 32 and columns (o / 32 / 4) * 64 + bit).
+__device__ __forceinline__ int pair_row(int o) { return ((o / kWarp) % 4) * kWarp + (o % kWarp); }
+__device__ __forceinline__ int pair_col(int o, int bit) { return ((o / kWarp) / 4) * 64 + bit; }
 
 // rows[r] (r < count and ids[r] != kNone, else zeros) minus `centre`, into a
 // chunk-major tile of `rows` rows (a multiple of 8).  Lane l of a warp
@@ -472,7 +549,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     uint32_t* fullrow = reinterpret_cast<uint32_t*>(smem + S.fullrow);
     float* centre = reinterpret_cast<float*>(smem + S.centre);
     unsigned long long* todo_s = reinterpret_cast<unsigned long long*>(smem + S.x);   // [kJoinThreads]
-    uint32_t* pref = reinterpret_cast<uint32_t*>(smem + S.x + kJoinThreads * 8);      // [kJoinThreads + 1]
+    unsigned long long* mem_s = todo_s + kJoinThreads;                                // [kJoinThreads]
+    uint32_t* pref = reinterpret_cast<uint32_t*>(smem + S.x + 2 * kJoinThreads * 8);  // [kJoinThreads + 1]
     uint32_t* wsum = pref + kJoinThreads + 1;                                          // [8]
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
@@ -665,97 +743,79 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                     }
                     todo |= static_cast<unsigned long long>(pass) << (cc * 16);
                 }
-                // Members of S(p) are rejected by the set update: drop them.
-                // Lower bounds of four candidates at a time (branch-free, in
-                // lockstep); a set that is not full lists its empty slots as
-                // id 0, which is not taken for a member.
-                const uint32_t* mylist = reinterpret_cast<const uint32_t*>(A) + row * KS;
-                const bool full = row < static_cast<int>(m) && fullrow[row] != 0u;
-                unsigned long long scan = todo;
+            }
+            // Filter-passing pairs of the block, then the members of S(p)
+            // among them (rejected by the set update: dropped), an even share
+            // of the pairs per thread, lower bounds of four at a time
+            // (branch-free, in lockstep).  A set that is not full lists its
+            // empty slots as id 0, which is not taken for a member.
+            todo_s[tid] = todo;
+            mem_s[tid] = 0ull;
+            uint32_t incl = scan_masks_warp(todo, wsum);
+            tc::fence_before_sync();
+            __syncthreads();
+            scan_masks_block(todo, incl, wsum, pref);
+            __syncthreads();
+            {
+                const uint32_t* lists = reinterpret_cast<const uint32_t*>(A);
+                PairCursor cur = pair_share(pref, todo_s);
 #pragma unroll 1
-                while (scan) {
-                    int bit[4];
+                while (cur.lo < cur.hi) {
+                    int own[4], bit[4], pos[4];
                     uint32_t key[4];
-                    int pos[4];
+                    const uint32_t* lst[4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        bit[u] = -1;
+                        own[u] = -1;
+                        bit[u] = 0;
                         key[u] = 0;
                         pos[u] = 0;
-                        if (scan) {
-                            bit[u] = __ffsll(scan) - 1;
-                            scan &= scan - 1;
-                            key[u] = cid[half * 64 + bit[u]];
+                        lst[u] = lists;
+                        if (cur.lo < cur.hi) {
+                            pair_next(cur, todo_s, own[u], bit[u]);
+                            key[u] = cid[pair_col(own[u], bit[u])];
+                            lst[u] = lists + pair_row(own[u]) * KS;
                         }
                     }
                     for (int step = search_top; step > 0; step >>= 1) {
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
                             const int t = pos[u] + step;
-                            if (t <= K && mylist[t - 1] < key[u]) pos[u] = t;
+                            if (t <= K && lst[u][t - 1] < key[u]) pos[u] = t;
                         }
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        if (bit[u] >= 0 && pos[u] < K && mylist[pos[u]] == key[u] && (key[u] != 0 || full)) {
-                            todo &= ~(1ull << bit[u]);
+                        if (own[u] >= 0 && pos[u] < K && lst[u][pos[u]] == key[u] &&
+                            (key[u] != 0 || fullrow[pair_row(own[u])] != 0u)) {
+                            atomicOr(&mem_s[own[u]], 1ull << bit[u]);
                             ++n_member;
                         }
                     }
                 }
             }
-            tc::fence_before_sync();
             __syncthreads();
-            // Pair masks and their block-wide prefix sums, then the original
-            // FP32 rows in the tiles' space.
+            // The remaining pairs and their prefix sums, then the original
+            // FP32 rows in the tiles' space (the lists are consumed).
+            todo &= ~mem_s[tid];
+            incl = scan_masks_warp(todo, wsum);
             todo_s[tid] = todo;
-            uint32_t x = static_cast<uint32_t>(__popcll(todo));
-#pragma unroll
-            for (int o = 1; o < kWarp; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(kFull, x, o);
-                if (lane >= o) x += y;
-            }
-            if (lane == kWarp - 1) wsum[warp] = x;
             float* Aorig = A;
             float* Bo = B;
             stage_rows<D>(Aorig, pid, m, pts, ld);
             stage_rows<D>(Bo, cid, nc, pts, ld);
             __syncthreads();
-            {
-                uint32_t before = 0, total = 0;
-#pragma unroll
-                for (int w = 0; w < kJoinThreads / kWarp; ++w) {
-                    const uint32_t s = wsum[w];
-                    before += w < warp ? s : 0u;
-                    total += s;
-                }
-                pref[tid] = before + x - static_cast<uint32_t>(__popcll(todo));
-                if (tid == 0) pref[kJoinThreads] = total;
-            }
+            scan_masks_block(todo, incl, wsum, pref);
             __syncthreads();
-            // Exact distances: pair indices [tid*T/256, (tid+1)*T/256) of the
-            // block's T pairs, in owner-thread then column order.
-            const uint32_t T = pref[kJoinThreads];
-            uint32_t lo = static_cast<uint32_t>((static_cast<unsigned long long>(tid) * T) / kJoinThreads);
-            const uint32_t hi = static_cast<uint32_t>((static_cast<unsigned long long>(tid + 1) * T) / kJoinThreads);
-            if (lo < hi) {
-                // Owner: the last thread o with pref[o] <= lo.
-                int a = 0, b = kJoinThreads - 1;
-                while (a < b) {
-                    const int mid = (a + b + 1) >> 1;
-                    if (pref[mid] <= lo) a = mid; else b = mid - 1;
-                }
-                int o = a;
-                unsigned long long bits = todo_s[o];
-                for (uint32_t r = lo - pref[o]; r > 0; --r) bits &= bits - 1;
+            // Exact distances over an even share of the remaining pairs.
+            {
+                PairCursor cur = pair_share(pref, todo_s);
 #pragma unroll 1
-                for (; lo < hi; ++lo) {
-                    while (bits == 0) bits = todo_s[++o];
-                    const int bit = __ffsll(bits) - 1;
-                    bits &= bits - 1;
-                    const int ow = o / kWarp;
-                    const int prow = (ow % 4) * kWarp + (o % kWarp);
-                    const int j = (ow / 4) * 64 + bit;
+                while (cur.lo < cur.hi) {
+                    int o, bit;
+                    pair_next(cur, todo_s, o, bit);
+                    const int prow = pair_row(o);
+                    const int j = pair_col(o, bit);
                     const uint32_t pp = pid[prow];
                     const uint32_t c = cid[j];
                     if (c == pp) continue;
