@@ -325,10 +325,11 @@ __host__ __device__ inline JoinSmem join_smem(int D, uint32_t K) {
     return s;
 }
 
-// Row stride (in ids) of the staged sorted lists: odd, so that the threads of
-// a warp (one row each) search on distinct banks, when 128 such rows fit in
-// the tiles' space.
+// Row stride (in ids) of the staged sorted lists: k when k is a multiple of 4
+// (rows copied in 16-byte pieces), else odd when 128 such rows fit in the
+// tiles' space (searches by different rows spread over the banks).
 __host__ __device__ inline int list_stride(int D, uint32_t K) {
+    if ((K & 3u) == 0) return static_cast<int>(K);
     const uint32_t KP = (D + 7) / 8 * 8;
     const uint32_t space = (kTile + join_cols(K)) * KP * 4;
     return static_cast<uint32_t>(kTile) * (K | 1u) * 4 <= space ? static_cast<int>(K | 1u) : static_cast<int>(K);
@@ -411,10 +412,11 @@ __device__ __forceinline__ int pair_row(int o) { return ((o / kWarp) % 4) * kWar
 __device__ __forceinline__ int pair_col(int o, int bit) { return ((o / kWarp) / 4) * 64 + bit; }
 
 // rows[r] (r < count and ids[r] != kNone, else zeros) minus `centre`, into a
-// chunk-major tile of `rows` rows (a multiple of 8).  Lane l of a warp
-// handles row (8g + l % 8), chunk (4h + l / 8): every global sector read is
-// used whole and each quarter-warp's 16-byte shared stores land on distinct
-// banks.
+// chunk-major tile of `rows` rows (a multiple of 8).  Every 16-byte chunk a
+// thread owns is first copied with cp.async (all of them in flight at once),
+// then centred in place by the same thread.  Lane l of a warp handles row
+// (8g + l % 8), chunk (4h + l / 8): every global sector read is used whole
+// and each quarter-warp's 16-byte shared accesses land on distinct banks.
 template <int D>
 __device__ __forceinline__ void stage_centred(float* __restrict__ tile, uint32_t rows, const uint32_t* __restrict__ ids,
                                               uint32_t count, const float* __restrict__ pts, int ld,
@@ -422,11 +424,11 @@ __device__ __forceinline__ void stage_centred(float* __restrict__ tile, uint32_t
     constexpr int CH = JoinLayout<D>::CH;
     constexpr int CG = (CH + 3) / 4;  // chunk groups
     constexpr int WARPS = kJoinThreads / kWarp;
-    constexpr int BATCH = 4;
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     const int rl = lane & 7, cl = lane >> 3;
     const int groups = static_cast<int>(rows / 8);
     const int tasks = groups * CG;
+    unsigned char* base = reinterpret_cast<unsigned char*>(tile);
     // Task w = (chunk group w / groups, row group w % groups); this warp's
     // tasks are warp, warp + WARPS, ...: the pair is advanced, not divided.
     int g = warp, cg = 0;
@@ -434,43 +436,37 @@ __device__ __forceinline__ void stage_centred(float* __restrict__ tile, uint32_t
         g -= groups;
         ++cg;
     }
+    const int g0 = g, cg0 = cg;
 #pragma unroll 1
-    for (int t0 = warp; t0 < tasks; t0 += BATCH * WARPS) {
-        float4 v[BATCH];
-        int tr[BATCH], tch[BATCH];
-#pragma unroll
-        for (int bi = 0; bi < BATCH; ++bi) {
-            tr[bi] = g * 8 + rl;
-            tch[bi] = cg * 4 + cl;
-            g += WARPS;
-            while (g >= groups) {
-                g -= groups;
-                ++cg;
-            }
+    for (int w = warp; w < tasks; w += WARPS) {
+        const int r = g * 8 + rl, ch = cg * 4 + cl;
+        if (ch < CH) {
+            const bool valid = static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone;
+            const float* src = valid ? pts + static_cast<size_t>(ids[r]) * ld + 4 * ch : pts;
+            tc::cp_async16(base + tc::chunk_offset(r, 4 * ch, rows), src, valid);
         }
-        // A batch of loads is issued before its stores.
-#pragma unroll
-        for (int bi = 0; bi < BATCH; ++bi) {
-            const int w = t0 + bi * WARPS;
-            const int r = tr[bi], ch = tch[bi];
-            v[bi] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (w < tasks && ch < CH && static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone)
-                v[bi] = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + ch);
+        g += WARPS;
+        while (g >= groups) {
+            g -= groups;
+            ++cg;
         }
-#pragma unroll
-        for (int bi = 0; bi < BATCH; ++bi) {
-            const int w = t0 + bi * WARPS;
-            const int r = tr[bi], ch = tch[bi];
-            if (w < tasks && ch < CH) {
-                float4 x = v[bi];
-                if (static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
-                    const float4 m = reinterpret_cast<const float4*>(centre)[ch];
-                    x = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z),
-                                    __fsub_rn(x.w, m.w));
-                }
-                *reinterpret_cast<float4*>(reinterpret_cast<unsigned char*>(tile) + tc::chunk_offset(r, 4 * ch, rows)) =
-                    x;
-            }
+    }
+    tc::cp_async_wait_all();
+    g = g0;
+    cg = cg0;
+#pragma unroll 1
+    for (int w = warp; w < tasks; w += WARPS) {
+        const int r = g * 8 + rl, ch = cg * 4 + cl;
+        if (ch < CH && static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
+            float4* at = reinterpret_cast<float4*>(base + tc::chunk_offset(r, 4 * ch, rows));
+            const float4 x = *at;
+            const float4 m = reinterpret_cast<const float4*>(centre)[ch];
+            *at = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z), __fsub_rn(x.w, m.w));
+        }
+        g += WARPS;
+        while (g >= groups) {
+            g -= groups;
+            ++cg;
         }
     }
 }
@@ -490,27 +486,24 @@ __device__ __forceinline__ float tile_norm(const float* __restrict__ tile, int r
 }
 
 // Copies rows ids[r] (r < count, ids[r] != kNone) into a row-major tile of D
-// floats per row; every load of a thread is issued before its stores.
+// floats per row with cp.async (all of a thread's copies in flight at once);
+// the caller waits (cp_async_wait_all, then a barrier).
 template <int D>
 __device__ __forceinline__ void stage_rows(float* __restrict__ dst, const uint32_t* __restrict__ ids, uint32_t count,
                                            const float* __restrict__ pts, int ld) {
     constexpr int Q = D / 4;
-    constexpr int BATCH = 4;
     const uint32_t total = count * Q;
+    uint32_t r = threadIdx.x / Q, q = threadIdx.x % Q;
+    constexpr uint32_t dr = kJoinThreads / Q, dq = kJoinThreads % Q;
 #pragma unroll 1
-    for (uint32_t f0 = threadIdx.x; f0 < total; f0 += BATCH * kJoinThreads) {
-        float4 v[BATCH];
-#pragma unroll
-        for (int bi = 0; bi < BATCH; ++bi) {
-            const uint32_t f = f0 + bi * kJoinThreads;
-            const uint32_t r = f / Q, q = f % Q;
-            if (f < total && ids[r] != kNone)
-                v[bi] = __ldg(reinterpret_cast<const float4*>(pts + static_cast<size_t>(ids[r]) * ld) + q);
-        }
-#pragma unroll
-        for (int bi = 0; bi < BATCH; ++bi) {
-            const uint32_t f = f0 + bi * kJoinThreads;
-            if (f < total && ids[f / Q] != kNone) reinterpret_cast<float4*>(dst)[f] = v[bi];
+    for (uint32_t f = threadIdx.x; f < total; f += kJoinThreads) {
+        const uint32_t id = ids[r];
+        if (id != kNone) tc::cp_async16(dst + static_cast<size_t>(f) * 4, pts + static_cast<size_t>(id) * ld + 4 * q, true);
+        r += dr;
+        q += dq;
+        if (q >= static_cast<uint32_t>(Q)) {
+            q -= Q;
+            ++r;
         }
     }
 }
@@ -646,35 +639,24 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                 uint32_t* dst = reinterpret_cast<uint32_t*>(A);
                 const uint32_t total = m * static_cast<uint32_t>(K);
                 if ((K & 3) == 0) {
-                    // 16-byte loads, a batch of eight in flight per thread.
+                    // 16-byte cp.async pieces (row stride KS = K), all in flight.
                     const uint32_t KV = static_cast<uint32_t>(K) / 4, tv = total / 4;
+                    uint32_t r = static_cast<uint32_t>(tid) / KV, a = static_cast<uint32_t>(tid) % KV;
+                    const uint32_t dr = kJoinThreads / KV, da = kJoinThreads % KV;
 #pragma unroll 1
-                    for (uint32_t f0 = tid; f0 < tv; f0 += 8 * kJoinThreads) {
-                        uint4 v[8];
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            const uint32_t f = f0 + u * kJoinThreads;
-                            v[u] = make_uint4(kNone, kNone, kNone, kNone);
-                            if (f < tv) {
-                                const uint32_t r = f / KV, a = f - r * KV;
-                                const uint32_t pr = pid[r];
-                                if (pr != kNone)
-                                    v[u] = __ldg(reinterpret_cast<const uint4*>(snap + static_cast<size_t>(pr) * K) + a);
-                            }
-                        }
-#pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            const uint32_t f = f0 + u * kJoinThreads;
-                            if (f < tv) {
-                                const uint32_t r = f / KV, a = 4 * (f - r * KV);
-                                uint32_t* d = dst + r * KS + a;
-                                d[0] = v[u].x;
-                                d[1] = v[u].y;
-                                d[2] = v[u].z;
-                                d[3] = v[u].w;
-                            }
+                    for (uint32_t f = tid; f < tv; f += kJoinThreads) {
+                        const uint32_t pr = pid[r];
+                        if (pr != kNone)
+                            tc::cp_async16(dst + static_cast<size_t>(f) * 4,
+                                           snap + static_cast<size_t>(pr) * K + 4 * a, true);
+                        r += dr;
+                        a += da;
+                        if (a >= KV) {
+                            a -= KV;
+                            ++r;
                         }
                     }
+                    tc::cp_async_wait_all();
                 } else {
 #pragma unroll 1
                     for (uint32_t f0 = tid; f0 < total; f0 += 4 * kJoinThreads) {
@@ -804,6 +786,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
             float* Bo = B;
             stage_rows<D>(Aorig, pid, m, pts, ld);
             stage_rows<D>(Bo, cid, nc, pts, ld);
+            tc::cp_async_wait_all();
             __syncthreads();
             scan_masks_block(todo, incl, wsum, pref);
             __syncthreads();
