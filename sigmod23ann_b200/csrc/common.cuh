@@ -179,11 +179,6 @@ __device__ __forceinline__ float canonical_distance4_lean(const float4* __restri
 //
 // Tie order of getMaxIdx: among slots holding the maximum distance, the one
 // with the smallest (slot % 8), then the smallest (slot / 8).
-__device__ __forceinline__ uint32_t tie_key(uint32_t slot) { return ((slot & 7u) << 8) | (slot >> 3); }
-
-__device__ __forceinline__ bool beats(float v, uint32_t s, float bv, uint32_t bs) {
-    return v > bv || (v == bv && tie_key(s) < tie_key(bs));
-}
 
 struct WarpSet {
     float dist[kSlotsPerLane];
@@ -229,32 +224,31 @@ __device__ __forceinline__ void set_store(const WarpSet& s, float* __restrict__ 
 }
 
 // Slot of the maximum distance over K filled slots, in getMaxIdx's tie order;
-// sets s.maxslot and s.bound (warp-uniform).
+// sets s.maxslot and s.bound (warp-uniform).  Distances are sums of squares
+// (+0 or positive), so their bit patterns order like their values: one warp
+// max reduction finds the largest distance, a second one, over the slots
+// holding it, the winner of the tie order (smallest slot % 8, then slot / 8,
+// encoded so that the preferred slot has the largest key).
 __device__ __forceinline__ void warp_argmax(WarpSet& s, int K, int lane) {
-    float bv = -1.0f;
-    uint32_t bs = kNone;
+    uint32_t vb = 0;
 #pragma unroll
     for (int r = 0; r < kSlotsPerLane; ++r) {
         const uint32_t slot = lane + r * kWarp;
-        if (slot < static_cast<uint32_t>(K) && (bs == kNone || beats(s.dist[r], slot, bv, bs))) {
-            bv = s.dist[r];
-            bs = slot;
-        }
+        if (slot < static_cast<uint32_t>(K)) vb = max(vb, __float_as_uint(s.dist[r]));
     }
+    const uint32_t top = __reduce_max_sync(kFull, vb);
+    uint32_t tk = 0;  // 128 - (slot % 8 * 16 + slot / 8) for slots holding `top`, else 0
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        float ov = __shfl_xor_sync(kFull, bv, off);
-        uint32_t os = __shfl_xor_sync(kFull, bs, off);
-        if (os != kNone && (bs == kNone || beats(ov, os, bv, bs))) {
-            bv = ov;
-            bs = os;
-        }
+    for (int r = 0; r < kSlotsPerLane; ++r) {
+        const uint32_t slot = lane + r * kWarp;
+        if (slot < static_cast<uint32_t>(K) && __float_as_uint(s.dist[r]) == top)
+            tk = max(tk, 128u - (((slot & 7u) << 4) | (slot >> 3)));
     }
-    s.maxslot = bs;
-    s.bound = bv;
+    const uint32_t t = 128u - __reduce_max_sync(kFull, tk);
+    s.maxslot = (t & 15u) * 8u + (t >> 4);
+    s.bound = __uint_as_float(top);
 }
 
-// True if cand is among the filled slots (warp-uniform result).
 __device__ __forceinline__ bool set_contains(const WarpSet& s, uint32_t cand, int lane) {
     bool hit = false;
 #pragma unroll
