@@ -43,7 +43,7 @@ DIM = 100
 K = 100
 MAX_LEAF = 1025        # buckets of at most 1024 points (leaf iff size < max_leaf)
 LLOYD_ITERS = 2
-REPS = 3
+REPS = 4
 REFINE = 2
 SEED = 1
 QUERIES = 10_000
