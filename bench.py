@@ -358,8 +358,13 @@ def run_ours(args):
         per_launch_ms = join_ms / max(1, join_launches)
         bytes_per_launch = (2.0 * n * K * DIM * 4) + (1.0 * n * K * K * 4)
         achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
+        # DRAM bytes of one launch from the committed ncu capture (500k points:
+        # 55.56 GB read + write), scaled by the points processed.
+        traffic = 55.56e9 * n / 500_000
         roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": achieved / hbm_peak, "traffic": None,
+                    "frac": achieved / hbm_peak, "traffic": traffic,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_join launch "
+                                      "at 500k points (profiles/k_join_500k.md), scaled by n",
                     "kernel": "k_join (neighbour-of-neighbour local join, tcgen05 TF32 filter)",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)" if peaks else
                                    "fallback 6650 GB/s",
