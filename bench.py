@@ -364,7 +364,7 @@ def run_ours(args):
         roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                     "frac": achieved / hbm_peak, "traffic": traffic,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_join launch "
-                                      "at 500k points (profiles/k_join_500k.md), scaled by n",
+                                      "at 500k points (committed capture summary), scaled by n",
                     "kernel": "k_join (neighbour-of-neighbour local join, tcgen05 TF32 filter)",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)" if peaks else
                                    "fallback 6650 GB/s",
