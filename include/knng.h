@@ -46,7 +46,8 @@ typedef enum knng_status {
     KNNG_ERR_BUDGET = 4,           /* the request exceeds the context's HBM budget */
     KNNG_ERR_STATE = 5,            /* call out of order, e.g. no points loaded */
     KNNG_ERR_UNSUPPORTED = 6,      /* d or k outside the compiled set */
-    KNNG_ERR_NO_DEVICE = 7         /* no CUDA device, or the device is not sm_100 */
+    KNNG_ERR_NO_DEVICE = 7,        /* no CUDA device, or the device is not sm_100 */
+    KNNG_ERR_PENDING = 8           /* a served job has not ended yet */
 } knng_status;
 
 enum {
@@ -240,6 +241,66 @@ knng_status knng_debug_tile_gram(knng_context* ctx, const float* a, uint32_t m, 
 knng_status knng_refine_pointwise_noalloc(const float* d_points, uint32_t n, uint32_t d, uint32_t k,
                                           uint32_t* d_snapshot, float* d_dist, uint32_t* d_ids, uint32_t* d_size,
                                           uint32_t* d_maxslot, float* d_bound, uint32_t* d_changed, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Serving form.  No counterpart in the reference, which builds one graph per
+ * process (constructResult, src/SolutionKmeans.hpp:558, called once from
+ * src/main.cpp:59).  A server owns one device and an HBM budget and accepts
+ * build jobs of different sizes as they arrive.  Jobs are admitted in arrival
+ * order while the admitted jobs' reservations (knng_job_reservation) fit the
+ * budget and fewer than max_running run; each admitted job builds on its own
+ * context and stream, so concurrent jobs overlap on the device, and its
+ * points and neighbour sets stay resident until its result is copied out.
+ * A job runs exactly the build of knng_build with the same parameters: its
+ * result is the same alone and among other jobs.
+ * ------------------------------------------------------------------------ */
+typedef struct knng_server knng_server;
+
+enum { KNNG_JOB_QUEUED = 0, KNNG_JOB_RUNNING = 1, KNNG_JOB_DONE = 2, KNNG_JOB_FAILED = 3 };
+
+typedef struct knng_job_info {
+    uint32_t state;           /* KNNG_JOB_* */
+    int32_t status;           /* knng_status of the build once ended */
+    uint32_t n, d, k;
+    uint32_t reserved0;
+    uint64_t reserved_bytes;  /* HBM reserved for the job while it runs */
+    double ms_queued;         /* submission to admission (so far, if still queued) */
+    double ms_run;            /* admission to end (so far, if running) */
+    double ms_latency;        /* submission to end (so far, if not ended) */
+    knng_stats stats;         /* the build's statistics once done */
+} knng_job_info;
+
+/* HBM a job of n points, d dims, k neighbours reserves: points, order, sets,
+ * refinement lists and survivor storage, plus fixed scratch. */
+uint64_t knng_job_reservation(uint32_t n, uint32_t d, uint32_t k);
+
+/* A server on `device` with an HBM budget (0: 80% of the device's memory) and
+ * up to max_running concurrent jobs. */
+knng_status knng_server_create(int device, uint64_t hbm_budget_bytes, uint32_t max_running, knng_server** out);
+
+/* Queues a job.  `points` (host, row stride ld_bytes), `out_ids` (n*k) and
+ * `out_dists` (n*k, nullable) must stay valid until the job has ended.
+ * KNNG_ERR_BUDGET if the job's reservation exceeds the whole budget. */
+knng_status knng_server_submit(knng_server* server, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                               const knng_params* params, uint32_t* out_ids, float* out_dists, uint64_t* out_job);
+
+/* Current state and timings of a job. */
+knng_status knng_server_poll(knng_server* server, uint64_t job, knng_job_info* info);
+
+/* Waits up to timeout_ms (< 0: without limit) for a job to end; KNNG_OK once
+ * it has ended (info.state and info.status tell how), KNNG_ERR_PENDING if not
+ * yet. */
+knng_status knng_server_wait(knng_server* server, uint64_t job, int64_t timeout_ms, knng_job_info* info);
+
+/* The error message of a failed job ("" otherwise). */
+const char* knng_server_job_error(knng_server* server, uint64_t job);
+
+/* Forgets an ended job's record (KNNG_ERR_PENDING if it has not ended). */
+knng_status knng_server_release(knng_server* server, uint64_t job);
+
+/* Refuses new jobs, cancels queued ones, waits for running ones, frees the
+ * server. */
+knng_status knng_server_destroy(knng_server* server);
 
 #ifdef __cplusplus
 }

@@ -4,11 +4,14 @@ buckets into bounded neighbour sets, neighbour-of-neighbour refinement -- all
 as sm_100a CUDA kernels behind the C ABI in include/knng.h."""
 from .api import (  # noqa: F401
     EXPORTED,
+    JobInfo,
     KnngContext,
     KnngError,
+    KnngServer,
     Params,
     Stats,
     construct_result,
     default_params,
+    job_reservation,
     load_library,
 )

@@ -22,7 +22,10 @@ KNNG_OK = 0
 STATUS_NAMES = {
     0: "KNNG_OK", 1: "KNNG_ERR_INVALID_ARGUMENT", 2: "KNNG_ERR_CUDA", 3: "KNNG_ERR_OUT_OF_MEMORY",
     4: "KNNG_ERR_BUDGET", 5: "KNNG_ERR_STATE", 6: "KNNG_ERR_UNSUPPORTED", 7: "KNNG_ERR_NO_DEVICE",
+    8: "KNNG_ERR_PENDING",
 }
+KNNG_ERR_PENDING = 8
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
 PRECISION_FP32 = 0
 PRECISION_BF16_RERANK = 1
 
@@ -33,6 +36,8 @@ EXPORTED = [
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
     "knng_debug_tile_gram", "knng_refine_pointwise_noalloc",
+    "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
+    "knng_server_job_error", "knng_server_release", "knng_server_destroy",
 ]
 
 
@@ -60,6 +65,14 @@ class Stats(Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class JobInfo(Structure):
+    _fields_ = [
+        ("state", c_uint32), ("status", c_int32), ("n", c_uint32), ("d", c_uint32), ("k", c_uint32),
+        ("reserved0", c_uint32), ("reserved_bytes", c_uint64), ("ms_queued", c_double), ("ms_run", c_double),
+        ("ms_latency", c_double), ("stats", Stats),
+    ]
 
 
 class KnngError(RuntimeError):
@@ -105,6 +118,15 @@ def load_library(path: str = LIB_PATH):
         "knng_finalize": (c_int, [P, P, P]),
         "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_refine_pointwise_noalloc": (c_int, [P, c_uint32, c_uint32, c_uint32, P, P, P, P, P, P, P, P]),
+        "knng_job_reservation": (c_uint64, [c_uint32, c_uint32, c_uint32]),
+        "knng_server_create": (c_int, [c_int, c_uint64, c_uint32, POINTER(c_void_p)]),
+        "knng_server_submit": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), P, P,
+                                       POINTER(c_uint64)]),
+        "knng_server_poll": (c_int, [P, c_uint64, POINTER(JobInfo)]),
+        "knng_server_wait": (c_int, [P, c_uint64, ctypes.c_int64, POINTER(JobInfo)]),
+        "knng_server_job_error": (c_char_p, [P, c_uint64]),
+        "knng_server_release": (c_int, [P, c_uint64]),
+        "knng_server_destroy": (c_int, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -318,3 +340,90 @@ def construct_result(points: np.ndarray, params: Params | None = None, device: i
     returns the n x k neighbour ids, sorted by (distance, id), short rows padded with id 1."""
     with KnngContext(device) as ctx:
         return ctx.build(points, params)
+
+
+class KnngServer:
+    """Serving form (knng_server_*): build jobs queued as they arrive, admitted
+    in arrival order within an HBM budget, up to `max_running` at once, each on
+    its own device context and stream.  A job's host buffers are held by this
+    object until the job is released."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_running: int = 4):
+        self._lib = load_library()
+        h = c_void_p()
+        st = self._lib.knng_server_create(device, hbm_budget_bytes, max_running, ctypes.byref(h))
+        if st != KNNG_OK:
+            raise KnngError(st, self._lib.knng_status_string(st).decode())
+        self._h = h
+        self._buffers: dict[int, tuple] = {}
+
+    def submit(self, points: np.ndarray, params: Params | None = None, want_dists: bool = False) -> int:
+        """Queues a build of `points` (n x d float32, rows may be strided);
+        returns the job id."""
+        pts = points if points.dtype == np.float32 and points.strides[1] == 4 else _f32(points)
+        n, d = pts.shape
+        p = params or default_params()
+        ids = np.empty((n, p.k), np.uint32)
+        dists = np.empty((n, p.k), np.float32) if want_dists else None
+        job = c_uint64()
+        st = self._lib.knng_server_submit(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p), _ptr(ids),
+                                          _ptr(dists), ctypes.byref(job))
+        if st != KNNG_OK:
+            raise KnngError(st, self._lib.knng_status_string(st).decode())
+        self._buffers[job.value] = (pts, p, ids, dists)
+        return job.value
+
+    def poll(self, job: int) -> JobInfo:
+        info = JobInfo()
+        st = self._lib.knng_server_poll(self._h, job, ctypes.byref(info))
+        if st != KNNG_OK:
+            raise KnngError(st, self._lib.knng_status_string(st).decode())
+        return info
+
+    def wait(self, job: int, timeout_ms: int = -1) -> JobInfo | None:
+        """The job's info once it has ended, or None after timeout_ms."""
+        info = JobInfo()
+        st = self._lib.knng_server_wait(self._h, job, timeout_ms, ctypes.byref(info))
+        if st == KNNG_ERR_PENDING:
+            return None
+        if st != KNNG_OK:
+            raise KnngError(st, self._lib.knng_status_string(st).decode())
+        return info
+
+    def result(self, job: int):
+        """(ids, dists or None) of an ended job; raises if it failed."""
+        info = self.wait(job)
+        if info.state != JOB_DONE:
+            msg = self._lib.knng_server_job_error(self._h, job)
+            raise KnngError(info.status, msg.decode() if msg else "")
+        _, _, ids, dists = self._buffers[job]
+        return ids, dists
+
+    def release(self, job: int) -> None:
+        st = self._lib.knng_server_release(self._h, job)
+        if st != KNNG_OK:
+            raise KnngError(st, self._lib.knng_status_string(st).decode())
+        self._buffers.pop(job, None)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.knng_server_destroy(self._h)
+            self._h = None
+            self._buffers.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def job_reservation(n: int, d: int, k: int) -> int:
+    """HBM bytes a served job of n points, d dims, k neighbours reserves."""
+    return int(load_library().knng_job_reservation(n, d, k))

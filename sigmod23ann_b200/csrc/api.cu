@@ -43,18 +43,21 @@ void check_cuda(cudaError_t e, const char* what) {
 
 bool dim_supported(uint32_t d) { return d == 64 || d == 100 || d == 128; }
 
+// Device memory is stream-ordered on the context's stream (all of the
+// context's work runs there), so allocating or freeing does not synchronise
+// the device under other contexts' work.
 void* dev_alloc(Context& c, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (c.held + bytes > c.budget) fail(KNNG_ERR_BUDGET, "device memory budget exceeded");
     void* p = nullptr;
-    check_cuda(cudaMalloc(&p, bytes), "cudaMalloc");
+    check_cuda(cudaMallocAsync(&p, bytes, c.stream), "cudaMallocAsync");
     c.held += bytes;
     return p;
 }
 
 void dev_free(Context& c, void* p, size_t bytes) {
     if (!p) return;
-    cudaFree(p);
+    cudaFreeAsync(p, c.stream);
     c.held -= std::min<uint64_t>(c.held, bytes == 0 ? 16 : bytes);
 }
 
@@ -517,6 +520,7 @@ const char* knng_status_string(knng_status s) {
         case KNNG_ERR_STATE: return "call out of order";
         case KNNG_ERR_UNSUPPORTED: return "unsupported dimension or k";
         case KNNG_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+        case KNNG_ERR_PENDING: return "job has not ended";
     }
     return "unknown status";
 }

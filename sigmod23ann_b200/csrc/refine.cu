@@ -1070,7 +1070,13 @@ void run_tile_gram(Context& c, uint32_t d, const float* d_a, uint32_t m, const f
 uint64_t run_refine_pointwise(Context& c, const uint32_t* snap, const uint32_t* d_list, uint32_t count) {
     const int K = static_cast<int>(c.k);
     const uint32_t cap = pow2_at_least(static_cast<uint32_t>(K * K));
-    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((count + kRefWarps - 1) / kRefWarps, 148 * 5));
+    uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((count + kRefWarps - 1) / kRefWarps, 148 * 5));
+    // Each block's warps need cap survivor keys; fewer blocks (a longer grid
+    // stride) when the budget leaves less room.
+    const uint64_t per_block = static_cast<uint64_t>(kRefWarps) * cap * sizeof(unsigned long long);
+    const uint64_t held_other = c.held - scratch_bytes(c, "refine_keys");
+    const uint64_t room = c.budget > held_other + (16ull << 20) ? c.budget - held_other - (16ull << 20) : 0;
+    blocks = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(blocks, room / per_block)));
     auto* keys = static_cast<unsigned long long*>(
         scratch(c, "refine_keys", static_cast<size_t>(blocks) * kRefWarps * cap * sizeof(unsigned long long)));
     auto* changed = static_cast<uint32_t*>(scratch(c, "refine_changed", sizeof(uint32_t)));
@@ -1144,7 +1150,7 @@ uint64_t run_refine(Context& c) {
     // Survivor storage: `slots` per point, then per-CTA pool regions for the
     // rest, both sized from the free budget (counting what they already hold).
     const uint64_t held_other = c.held - scratch_bytes(c, "surv_direct") - scratch_bytes(c, "surv_pool");
-    const uint64_t reserve = (1ull << 30) + static_cast<uint64_t>(n) * 32;
+    const uint64_t reserve = std::min<uint64_t>(1ull << 30, c.budget / 8) + static_cast<uint64_t>(n) * 32;
     const uint64_t avail = c.budget > held_other + reserve ? c.budget - held_other - reserve : 0;
     uint32_t slots = 0;
     if (c.refine_slots >= 0) {
@@ -1236,9 +1242,16 @@ uint64_t run_refine(Context& c) {
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     if (max_count > static_cast<uint32_t>(kApplyCap)) {
-        auto* big_keys = static_cast<unsigned long long*>(scratch(
-            c, "apply_big_keys", static_cast<size_t>(kJoinBlocks) * kRefWarps * big_cap * sizeof(unsigned long long)));
-        k_apply_big<<<kJoinBlocks, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, slots, direct, soff, ovf,
+        // Each block's warps sort in big_cap keys of global scratch: fewer
+        // blocks (a longer grid stride) when the budget leaves less room.
+        const uint64_t per_block = static_cast<uint64_t>(kRefWarps) * big_cap * sizeof(unsigned long long);
+        const uint64_t held_other = c.held - scratch_bytes(c, "apply_big_keys");
+        const uint64_t room = c.budget > held_other + (16ull << 20) ? c.budget - held_other - (16ull << 20) : 0;
+        const uint32_t big_blocks =
+            static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(kJoinBlocks, room / per_block)));
+        auto* big_keys = static_cast<unsigned long long*>(
+            scratch(c, "apply_big_keys", static_cast<size_t>(big_blocks) * per_block));
+        k_apply_big<<<big_blocks, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, slots, direct, soff, ovf,
                                                                     big_keys, big_cap, c.set_dist, c.set_id,
                                                                     c.set_size, c.set_maxslot, c.set_bound,
                                                                     counters + 1);

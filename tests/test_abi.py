@@ -39,7 +39,7 @@ def test_default_params_are_the_references(knng_lib):
 
 
 def test_status_strings(knng_lib):
-    for code in range(8):
+    for code in range(9):
         assert knng_lib.knng_status_string(code)
     assert knng_lib.knng_status_string(0) == b"ok"
 
@@ -95,3 +95,27 @@ int main() {
         assert r.returncode == 0, r.stdout + r.stderr
     else:
         assert r.returncode == 3 and "no sm_100" in r.stdout, r.stdout + r.stderr
+
+
+def test_job_reservation_arithmetic(knng_lib):
+    """A served job reserves its points, order, sets, refinement lists and
+    survivor storage plus fixed scratch: linear in n, growing with d and k."""
+    from sigmod23ann_b200 import job_reservation
+
+    fixed = 256 << 20
+    r1 = job_reservation(1_000_000, 100, 100)
+    per_point = 100 * 4 + 8 + (100 * 8 + 12) + (100 * 8 + 40) + 100 * 96
+    assert r1 == fixed + 1_000_000 * per_point
+    assert job_reservation(2_000_000, 100, 100) - fixed == 2 * (r1 - fixed)
+    assert job_reservation(1_000_000, 128, 100) > r1 > job_reservation(1_000_000, 64, 100)
+    assert job_reservation(1_000_000, 100, 10) < r1
+
+
+def test_server_without_device_reports_no_device(knng_lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.KnngError) as e:
+        api.KnngServer(0)
+    assert e.value.status == 7
