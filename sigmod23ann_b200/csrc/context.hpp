@@ -104,6 +104,21 @@ void download(Context& c, T* host, const T* dev, size_t count) {
 
 bool dim_supported(uint32_t d);
 
+// Lets `kern` take as much dynamic shared memory as the device allows a block
+// (the opt-in maximum less the kernel's static shared memory).  The attribute
+// is process-wide per kernel, so contexts running concurrently must all set
+// the same value -- this maximum, not the size of one launch (each launch
+// passes its own size).
+template <class Kernel>
+void allow_max_smem(Context& c, Kernel kern) {
+    int optin = 0;
+    KNNG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+    cudaFuncAttributes fa{};
+    KNNG_CUDA(cudaFuncGetAttributes(&fa, kern));
+    KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   optin - static_cast<int>(fa.sharedSizeBytes)));
+}
+
 // ----------------------------------------------------------- launchers
 // split.cu
 void launch_iota(Context& c);

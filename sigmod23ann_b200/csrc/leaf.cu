@@ -161,7 +161,7 @@ void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const u
                             static_cast<size_t>(std::max<uint32_t>(max_bucket, 1)) * sizeof(uint32_t);
         if (smem > 227 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "bucket too large for the bucket kernel");
         auto kern = k_leaf<D>;
-        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_max_smem(c, kern);
         kern<<<count, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
                                                       c.set_id, c.set_size, c.set_maxslot, c.set_bound,
                                                       static_cast<int>(c.k));

@@ -1057,7 +1057,7 @@ void run_tile_gram(Context& c, uint32_t d, const float* d_a, uint32_t m, const f
     KNNG_DISPATCH_D(d, {
         const size_t smem = 2 * JoinLayout<D>::tile_bytes + kTile * 4 + D * 4;
         auto kern = k_tile_gram<D>;
-        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_max_smem(c, kern);
         kern<<<1, kJoinThreads, smem, c.stream>>>(d_a, m, d_b, n, d_out, err);
     });
     ++c.launches;
@@ -1136,7 +1136,7 @@ uint64_t run_refine(Context& c) {
     cudaFuncAttributes fa{};
     KNNG_DISPATCH_D(c.d, {
         auto kern = k_join<D>;
-        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(join_bytes)));
+        allow_max_smem(c, kern);
         KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        static_cast<int>(cudaSharedmemCarveoutMaxShared)));
         KNNG_CUDA(cudaFuncGetAttributes(&fa, kern));

@@ -435,7 +435,7 @@ void launch_farthest_pair(Context& c, uint32_t count, const uint64_t* d_offsets,
     if (smem > 200 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "farthest-pair list too long");
     KNNG_DISPATCH_D(c.d, {
         auto kern = k_farthest_pair<D>;
-        KNNG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_max_smem(c, kern);
         kern<<<count, kPairThreads, smem, c.stream>>>(d_offsets, d_positions, c.indices, c.points, c.ld, d_first,
                                                       d_second, d_ok, d_c1, d_c2);
     });
