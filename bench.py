@@ -65,6 +65,8 @@ def parse_args(argv=None):
     ap.add_argument("--serving-requests", type=int, default=24,
                     help="requests of the serving stream measured beside the build (0: skip)")
     ap.add_argument("--serving", action="store_true", help="measure only the serving stream")
+    ap.add_argument("--batched", action="store_true", help="measure only the batched form (4,096 sets, 5 waves)")
+    ap.add_argument("--batched-waves", type=int, default=5, help="waves of the batched form to run (of 5)")
     return ap.parse_args(argv)
 
 
@@ -346,6 +348,80 @@ def run_serving(requests: int, device: int = 0, max_running: int = 4) -> dict:
     }
 
 
+# ------------------------------------------------------------ batched arm
+
+def batched_sets(seed: int = 2, count: int = 4096):
+    """Sizes of the batched form: log-uniform in [1e3, 2e5] (seed 2)."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(1e3), np.log(2e5), size=count)).astype(np.int64)
+
+
+def batched_wave_points(sizes, wave_seed: int, device: str):
+    """One wave's sets, concatenated: each set a mixture of 16 Gaussians
+    (sigma 0.2, centres uniform in [-1,1]^100, equal weights)."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(wave_seed)
+    s = len(sizes)
+    centres = torch.rand((s, 16, DIM), generator=g, device=device) * 2.0 - 1.0
+    set_of = torch.repeat_interleave(torch.arange(s, device=device), torch.as_tensor(sizes, device=device))
+    label = torch.randint(0, 16, (int(sizes.sum()),), generator=g, device=device)
+    x = centres[set_of, label] + 0.2 * torch.randn((int(sizes.sum()), DIM), generator=g, device=device)
+    return x.contiguous()
+
+
+def run_batched(waves: int, device: int = 0) -> dict:
+    """Batched form: 4,096 independent sets (about 160M points) in 5 waves of
+    about 820 sets; each wave is one knng_build_batch on device-resident
+    points (every tree level, bucket pass and join shared by the wave's sets).
+    points/s = points built / device time (CUDA events on the library's
+    stream).  Recall on 1k sampled points of 16 sampled sets per wave."""
+    import torch
+
+    from sigmod23ann_b200 import KnngContext, Stats, default_params, groundtruth
+    from sigmod23ann_b200.api import _ptr
+
+    sizes = batched_sets()
+    per_wave = np.array_split(np.arange(len(sizes)), 5)
+    params = default_params(k=K, max_leaf=MAX_LEAF, max_leaf_odd=0, lloyd_iters=LLOYD_ITERS, reps=REPS,
+                            refine=REFINE, seed=SEED)
+    dev = f"cuda:{device}"
+    ctx = KnngContext(device)
+    total_points, total_ms, recalls, waves_out = 0, 0.0, [], []
+    lib = ctx._lib
+    import ctypes
+
+    for w in range(min(waves, 5)):
+        ws = sizes[per_wave[w]]
+        x = batched_wave_points(ws, 100 + w, dev)
+        offs = np.zeros(len(ws) + 1, np.uint32)
+        offs[1:] = np.cumsum(ws)
+        n = int(offs[-1])
+        ids = torch.empty((n, K), dtype=torch.int32, device=dev)
+        st = Stats()
+        ctx._check(lib.knng_build_batch(ctx._h, _ptr(x), n, DIM, DIM * 4, _ptr(offs), len(ws), 1,
+                                        ctypes.byref(params), _ptr(ids), None, ctypes.byref(st)))
+        ms = st.ms_total + st.ms_finalize
+        total_points += n
+        total_ms += ms
+        rng = np.random.default_rng(w)
+        for s in rng.choice(len(ws), 16, replace=False):
+            a, b = int(offs[s]), int(offs[s + 1])
+            q = rng.choice(b - a, min(1000, b - a), replace=False)
+            gt = groundtruth.exact_knn_torch(x[a:b], q, K)
+            recalls.append(groundtruth.recall(ids[a:b].cpu().numpy().view(np.uint32).astype(np.int64), gt, q))
+        waves_out.append({"sets": len(ws), "points": n, "ms": ms})
+        del x, ids
+        torch.cuda.empty_cache()
+    ctx.close()
+    return {"sets": int(sum(w["sets"] for w in waves_out)), "points": total_points, "ms": total_ms,
+            "points_per_s": total_points / (total_ms / 1000.0), "waves": waves_out,
+            "min_recall": float(min(recalls)), "mean_recall": float(np.mean(recalls)),
+            "workload": "4,096 sets (seed 2), sizes log-uniform [1e3, 2e5], 16-Gaussian mixtures (sigma 0.2), "
+                        "d=100, k=100, 5 waves; FP32 distances, 4 repetitions + 2 passes per set"}
+
+
 # ------------------------------------------------------------ our arm
 
 def run_ours(args):
@@ -501,6 +577,12 @@ def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.batched:
+        res = run_batched(args.batched_waves)
+        print(json.dumps({"metric": "points/sec, batched k-NN graph builds (4,096 sets)", "value": res["points_per_s"],
+                          "unit": "points/s", "higher_is_better": True, "n_gpus": 1, "dtype": "f32",
+                          "batched": res}))
+        return 0
     if args.serving:
         res = run_serving(max(1, args.serving_requests))
         print(json.dumps({"metric": "p50/p99 latency of k-NN graph build jobs (serving stream)",

@@ -242,6 +242,22 @@ knng_status knng_refine_pointwise_noalloc(const float* d_points, uint32_t n, uin
                                           uint32_t* d_snapshot, float* d_dist, uint32_t* d_ids, uint32_t* d_size,
                                           uint32_t* d_maxslot, float* d_bound, uint32_t* d_changed, void* stream);
 
+/* Batched form: many independent point sets in one build.  No counterpart in
+ * the reference (one constructResult per process); each set is built as
+ * knng_build would build it alone, with the same parameters and result, but
+ * all sets share every launch: one set of launches per tree level across all
+ * sets' nodes, one bucket launch per repetition across all sets' buckets, one
+ * join per refinement pass.
+ *   points       n rows (all sets concatenated), row stride ld_bytes
+ *   set_offsets  n_sets + 1 ascending offsets, [0] = 0, [n_sets] = n; set s is
+ *                rows [set_offsets[s], set_offsets[s+1]), at least one row
+ *   on_device    nonzero: points, out_ids and out_dists are device pointers
+ *   out_ids      n x k ids relative to each row's set (padding id 1 as in
+ *                knng_build) */
+knng_status knng_build_batch(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                             const uint32_t* set_offsets, uint32_t n_sets, int on_device, const knng_params* params,
+                             uint32_t* out_ids, float* out_dists, knng_stats* stats);
+
 /* ------------------------------------------------------------------------
  * Serving form.  No counterpart in the reference, which builds one graph per
  * process (constructResult, src/SolutionKmeans.hpp:558, called once from

@@ -35,7 +35,7 @@ EXPORTED = [
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
-    "knng_debug_tile_gram", "knng_refine_pointwise_noalloc",
+    "knng_debug_tile_gram", "knng_refine_pointwise_noalloc", "knng_build_batch",
     "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
     "knng_server_job_error", "knng_server_release", "knng_server_destroy",
 ]
@@ -118,6 +118,8 @@ def load_library(path: str = LIB_PATH):
         "knng_finalize": (c_int, [P, P, P]),
         "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_refine_pointwise_noalloc": (c_int, [P, c_uint32, c_uint32, c_uint32, P, P, P, P, P, P, P, P]),
+        "knng_build_batch": (c_int, [P, P, c_uint32, c_uint32, c_uint64, P, c_uint32, c_int, POINTER(Params), P, P,
+                                     POINTER(Stats)]),
         "knng_job_reservation": (c_uint64, [c_uint32, c_uint32, c_uint32]),
         "knng_server_create": (c_int, [c_int, c_uint64, c_uint32, POINTER(c_void_p)]),
         "knng_server_submit": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), P, P,
@@ -217,6 +219,29 @@ class KnngContext:
                                          _ptr(dists), ctypes.byref(st)))
         self.n, self.d, self.k = n, d, p.k
         return (ids, dists) if want_dists else ids
+
+    def build_batch(self, sets, params: Params | None = None, want_dists: bool = False,
+                    stats: Stats | None = None):
+        """Builds every point set of `sets` (a list of n_s x d float32 arrays)
+        in one batched build; returns per-set id arrays (ids relative to the
+        set), and distance arrays when asked."""
+        arrays = [_f32(a) for a in sets]
+        offsets = np.zeros(len(arrays) + 1, np.uint32)
+        offsets[1:] = np.cumsum([a.shape[0] for a in arrays])
+        pts = np.ascontiguousarray(np.concatenate(arrays, axis=0))
+        n, d = pts.shape
+        p = params or default_params()
+        ids = np.empty((n, p.k), np.uint32)
+        dists = np.empty((n, p.k), np.float32) if want_dists else None
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_build_batch(self._h, _ptr(pts), n, d, pts.strides[0], _ptr(offsets),
+                                               len(arrays), 0, ctypes.byref(p), _ptr(ids), _ptr(dists),
+                                               ctypes.byref(st)))
+        self.n, self.d, self.k = n, d, p.k
+        out_ids = [ids[offsets[s]:offsets[s + 1]] for s in range(len(arrays))]
+        if not want_dists:
+            return out_ids
+        return out_ids, [dists[offsets[s]:offsets[s + 1]] for s in range(len(arrays))]
 
     def build_device(self, points_ptr: int, n: int, d: int, out_ids_ptr: int, out_dists_ptr: int | None = None,
                      params: Params | None = None, stats: Stats | None = None, ld_bytes: int = 0) -> Stats:

@@ -218,6 +218,8 @@ void load_points(Context& c, const float* pts, uint32_t n, uint32_t d, uint64_t 
             KNNG_CUDA(cudaMemcpy2DAsync(c.points, row, pts, ld_bytes, row, n,
                                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
     }
+    c.set_offsets = {0u, n};
+    c.d_set_offsets = nullptr;
     launch_iota(c);
 }
 
@@ -225,6 +227,7 @@ void load_points(Context& c, const float* pts, uint32_t n, uint32_t d, uint64_t 
 
 struct Node {
     uint32_t start, end;
+    uint32_t base;  // first id of the node's point set (RNG keys are relative to it)
 };
 
 struct RepStats {
@@ -261,7 +264,7 @@ std::vector<uint32_t> split_level(Context& c, const std::vector<Node>& active, u
         // Draw lists: large nodes draw their whole sample and seed from its
         // first min(|sample|, S) entries; small nodes draw S seeds and run
         // Lloyd over their whole range.
-        std::vector<uint32_t> hs(cnt), he(cnt), ha(cnt);
+        std::vector<uint32_t> hs(cnt), he(cnt), ha(cnt), hb(cnt);
         std::vector<uint64_t> draw_off(cnt + 1), seed_off(cnt + 1), lloyd_off(cnt + 1);
         uint64_t total = 0, seed_total = 0, lloyd_total = 0;
         uint32_t max_seed = 1;
@@ -270,6 +273,7 @@ std::vector<uint32_t> split_level(Context& c, const std::vector<Node>& active, u
             const uint32_t n = nd.end - nd.start;
             hs[t] = nd.start;
             he[t] = nd.end;
+            hb[t] = nd.base;
             ha[t] = attempt[todo[t]];
             const bool large = n >= small_threshold;
             const uint32_t S = start_count(n);
@@ -288,12 +292,13 @@ std::vector<uint32_t> split_level(Context& c, const std::vector<Node>& active, u
         uint32_t* d_s = upload(c, "lvl_start", hs.data(), cnt);
         uint32_t* d_e = upload(c, "lvl_end", he.data(), cnt);
         uint32_t* d_a = upload(c, "lvl_attempt", ha.data(), cnt);
+        uint32_t* d_b = upload(c, "lvl_base", hb.data(), cnt);
         uint64_t* d_doff = upload(c, "lvl_draw_off", draw_off.data(), cnt + 1);
         uint64_t* d_sb = upload(c, "lvl_seed_off", seed_off.data(), cnt + 1);
         uint64_t* d_loff = upload(c, "lvl_lloyd_off", lloyd_off.data(), cnt + 1);
         uint32_t* seeds = static_cast<uint32_t*>(scratch(c, "lvl_seeds", (seed_total + 1) * sizeof(uint32_t)));
         uint32_t* lloyd = static_cast<uint32_t*>(scratch(c, "lvl_lloyd", (lloyd_total + 1) * sizeof(uint32_t)));
-        launch_draw_positions(c, cnt, d_s, d_e, d_a, d_doff, d_sb, d_loff, seed, rep, seeds, lloyd);
+        launch_draw_positions(c, cnt, d_s, d_e, d_b, d_a, d_doff, d_sb, d_loff, seed, rep, seeds, lloyd);
         uint32_t* first = static_cast<uint32_t*>(scratch(c, "lvl_first", cnt * sizeof(uint32_t)));
         uint32_t* second = static_cast<uint32_t*>(scratch(c, "lvl_second", cnt * sizeof(uint32_t)));
         int32_t* ok = static_cast<int32_t*>(scratch(c, "lvl_ok", cnt * sizeof(int32_t)));
@@ -361,7 +366,9 @@ void run_rep(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small
     if (max_leaf < 2) fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be >= 2");
     EventPair split_t(c);
     launch_iota(c);
-    std::vector<Node> level{{0, c.n}};
+    std::vector<Node> level;
+    for (size_t s = 0; s + 1 < c.set_offsets.size(); ++s)
+        level.push_back({c.set_offsets[s], c.set_offsets[s + 1], c.set_offsets[s]});
     std::vector<Node> leaves;
     while (!level.empty()) {
         std::vector<Node> active;
@@ -377,8 +384,8 @@ void run_rep(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small
         std::vector<uint32_t> mids = split_level(c, active, lloyd_iters, small_threshold, seed, rep, st);
         level.clear();
         for (size_t i = 0; i < active.size(); ++i) {
-            level.push_back({active[i].start, mids[i]});
-            level.push_back({mids[i], active[i].end});
+            level.push_back({active[i].start, mids[i], active[i].base});
+            level.push_back({mids[i], active[i].end, active[i].base});
         }
     }
     st.ms_split += split_t.stop(c);
@@ -825,6 +832,43 @@ knng_status knng_build(knng_context* ctx, const float* points, uint32_t n, uint3
         if (stats) stats->ms_finalize += ft.stop(c);
         knng::download(c, out_ids, d_ids, nk);
         if (out_dists) knng::download(c, out_dists, d_dist, nk);
+    });
+}
+
+knng_status knng_build_batch(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                             const uint32_t* set_offsets, uint32_t n_sets, int on_device, const knng_params* params,
+                             uint32_t* out_ids, float* out_dists, knng_stats* stats) {
+    return knng::guarded(ctx, [&](Context& c) {
+        knng::validate_params(params);
+        if (!out_ids || !set_offsets) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null output or offsets");
+        if (n_sets == 0 || set_offsets[0] != 0 || set_offsets[n_sets] != n)
+            knng::fail(KNNG_ERR_INVALID_ARGUMENT, "set offsets must run from 0 to n");
+        for (uint32_t s = 0; s < n_sets; ++s)
+            if (set_offsets[s + 1] <= set_offsets[s]) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "empty or unordered set");
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        knng::load_points(c, points, n, d, ld_bytes, on_device != 0, on_device != 0);
+        c.set_offsets.assign(set_offsets, set_offsets + n_sets + 1);
+        if (n_sets > 1) c.d_set_offsets = knng::upload(c, "set_offsets", set_offsets, n_sets + 1);
+        knng::build_all(c, params, stats);
+        const size_t nk = static_cast<size_t>(c.n) * c.k;
+        knng::EventPair ft(c);
+        const uint64_t l0 = c.launches;
+        uint32_t* d_ids = on_device ? out_ids : static_cast<uint32_t*>(knng::scratch(c, "fin_ids", nk * sizeof(uint32_t)));
+        float* d_dist = on_device ? out_dists
+                                  : (out_dists ? static_cast<float*>(knng::scratch(c, "fin_dist", nk * sizeof(float)))
+                                               : nullptr);
+        knng::launch_finalize(c, d_ids, d_dist);
+        knng::launch_rebase_ids(c, d_ids);
+        if (stats) {
+            stats->ms_finalize += ft.stop(c);
+            stats->kernel_launches += c.launches - l0;
+        }
+        if (on_device) {
+            KNNG_CUDA(cudaStreamSynchronize(c.stream));
+        } else {
+            knng::download(c, out_ids, d_ids, nk);
+            if (out_dists) knng::download(c, out_dists, d_dist, nk);
+        }
     });
 }
 

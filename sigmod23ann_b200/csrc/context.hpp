@@ -48,6 +48,12 @@ struct Context {
     uint32_t* indices = nullptr;
     uint32_t* indices_tmp = nullptr;
 
+    // Independent point sets (batched builds): set s owns ids
+    // [set_offsets[s], set_offsets[s+1]); one set {0, n} otherwise.  Each set
+    // is its own tree root and its empty slots read as its first id.
+    std::vector<uint32_t> set_offsets;
+    uint32_t* d_set_offsets = nullptr;  // device copy when there is more than one set
+
     // Neighbour sets, slot order, capacity k per point.
     uint32_t k = 0;
     float* set_dist = nullptr;
@@ -126,7 +132,8 @@ void launch_iota(Context& c);
 // positions; the first seed-list-length of them go to d_seeds (CSR seed_off),
 // the first Lloyd-list-length to d_lloyd (CSR lloyd_off).
 void launch_draw_positions(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
-                           const uint32_t* d_attempts, const uint64_t* d_draw_off, const uint64_t* d_seed_off,
+                           const uint32_t* d_bases, const uint32_t* d_attempts, const uint64_t* d_draw_off,
+                           const uint64_t* d_seed_off,
                            const uint64_t* d_lloyd_off, uint64_t seed, uint32_t rep, uint32_t* d_seeds,
                            uint32_t* d_lloyd);
 // Dense copy of the hyperplanes of the picked nodes.
@@ -156,5 +163,7 @@ void run_tile_gram(Context& c, uint32_t d, const float* d_a, uint32_t m, const f
 // finalize.cu
 void launch_finalize(Context& c, uint32_t* d_ids, float* d_dists);
 void launch_reset_sets(Context& c);
+// Batched builds: output ids relative to each point's set (padding stays 1).
+void launch_rebase_ids(Context& c, uint32_t* d_ids);
 
 }  // namespace knng

@@ -730,7 +730,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
             // among them (rejected by the set update: dropped), an even share
             // of the pairs per thread, lower bounds of four at a time
             // (branch-free, in lockstep).  A set that is not full lists its
-            // empty slots as id 0, which is not taken for a member.
+            // empty slots as its point set's first id (0 for a single set),
+            // which is then its list's first entry and not taken for a member.
             todo_s[tid] = todo;
             mem_s[tid] = 0ull;
             uint32_t incl = scan_masks_warp(todo, wsum);
@@ -769,7 +770,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         if (own[u] >= 0 && pos[u] < K && lst[u][pos[u]] == key[u] &&
-                            (key[u] != 0 || fullrow[pair_row(own[u])] != 0u)) {
+                            (key[u] != lst[u][0] || fullrow[pair_row(own[u])] != 0u)) {
                             atomicOr(&mem_s[own[u]], 1ull << bit[u]);
                             ++n_member;
                         }

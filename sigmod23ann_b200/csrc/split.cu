@@ -51,8 +51,11 @@ __global__ void k_iota(uint32_t* __restrict__ idx, uint32_t n) {
 
 // Node i draws draws[i] positions; the first seed_len[i] go to its seed list
 // and the first lloyd_len[i] to its Lloyd list (both CSR).
+// Node [start, end) of a set starting at `base` draws with keys relative to
+// the set, so a set's tree is the same alone and in a batch.
 __global__ void k_draw_positions(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,
-                                 const uint32_t* __restrict__ attempts, const uint64_t* __restrict__ draw_off,
+                                 const uint32_t* __restrict__ bases, const uint32_t* __restrict__ attempts,
+                                 const uint64_t* __restrict__ draw_off,
                                  const uint64_t* __restrict__ seed_off, const uint64_t* __restrict__ lloyd_off,
                                  uint64_t seed, uint32_t rep, uint32_t* __restrict__ seeds_out,
                                  uint32_t* __restrict__ lloyd_out) {
@@ -60,9 +63,9 @@ __global__ void k_draw_positions(const uint32_t* __restrict__ starts, const uint
     const uint64_t cnt = draw_off[node + 1] - draw_off[node];
     const uint64_t sb = seed_off[node], sl = seed_off[node + 1] - sb;
     const uint64_t lb = lloyd_off[node], ll = lloyd_off[node + 1] - lb;
-    const uint32_t s = starts[node], t = ends[node], a = attempts[node];
+    const uint32_t s = starts[node], t = ends[node], a = attempts[node], b = bases[node];
     for (uint64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-        const uint32_t pos = counter_position(seed, rep, s, t, a, static_cast<uint32_t>(i));
+        const uint32_t pos = b + counter_position(seed, rep, s - b, t - b, a, static_cast<uint32_t>(i));
         if (i < sl) seeds_out[sb + i] = pos;
         if (i < ll) lloyd_out[lb + i] = pos;
     }
@@ -409,11 +412,11 @@ void launch_iota(Context& c) {
 }
 
 void launch_draw_positions(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
-                           const uint32_t* d_attempts, const uint64_t* d_draw_off, const uint64_t* d_seed_off,
-                           const uint64_t* d_lloyd_off, uint64_t seed, uint32_t rep, uint32_t* d_seeds,
-                           uint32_t* d_lloyd) {
+                           const uint32_t* d_bases, const uint32_t* d_attempts, const uint64_t* d_draw_off,
+                           const uint64_t* d_seed_off, const uint64_t* d_lloyd_off, uint64_t seed, uint32_t rep,
+                           uint32_t* d_seeds, uint32_t* d_lloyd) {
     if (count == 0) return;
-    k_draw_positions<<<count, 256, 0, c.stream>>>(d_starts, d_ends, d_attempts, d_draw_off, d_seed_off, d_lloyd_off,
+    k_draw_positions<<<count, 256, 0, c.stream>>>(d_starts, d_ends, d_bases, d_attempts, d_draw_off, d_seed_off, d_lloyd_off,
                                                   seed, rep, d_seeds, d_lloyd);
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());

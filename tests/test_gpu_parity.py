@@ -299,3 +299,19 @@ def test_budget_is_enforced(knng_lib):
         c.build(np.zeros((100_000, 100), np.float32))
     assert e.value.status == 4
     c.close()
+
+
+def test_batched_build_equals_builds_alone(knng_lib):
+    """Several independent point sets in one batched build give, per set, the
+    same ids and distances (bit for bit) as building each set alone -- a set
+    smaller than k + 1 (whose neighbour sets never fill) included."""
+    sizes = [3000, 1500, 50, 1200, 7000]
+    sets = [workloads.gaussian_mixture(n=m, d=100, clusters=6, sigma=0.2, seed=40 + i) for i, m in enumerate(sizes)]
+    params = default_params(reps=2, refine=1, max_leaf=257, max_leaf_odd=0, lloyd_iters=2, seed=77)
+    with KnngContext(0) as ctx:
+        b_ids, b_d = ctx.build_batch(sets, params, want_dists=True)
+    for s, pts in enumerate(sets):
+        with KnngContext(0) as ctx:
+            ids, dist = ctx.build(pts, params, want_dists=True)
+        assert np.array_equal(b_ids[s], ids), f"set {s} ids"
+        assert np.array_equal(b_d[s].view(np.uint32), dist.view(np.uint32)), f"set {s} distances"
