@@ -66,6 +66,8 @@ def parse_args(argv=None):
                     help="requests of the serving stream measured beside the build (0: skip)")
     ap.add_argument("--serving", action="store_true", help="measure only the serving stream")
     ap.add_argument("--batched", action="store_true", help="measure only the batched form (4,096 sets, 5 waves)")
+    ap.add_argument("--precision", action="store_true",
+                    help="measure only the precision form against the FP32 form (100k-point config)")
     ap.add_argument("--batched-waves", type=int, default=5, help="waves of the batched form to run (of 5)")
     return ap.parse_args(argv)
 
@@ -348,6 +350,74 @@ def run_serving(requests: int, device: int = 0, max_running: int = 4) -> dict:
     }
 
 
+# ------------------------------------------------------------ precision arm
+
+def run_precision(device: int = 0, steps: int = 3) -> dict:
+    """Precision form on the 100k-point config (64 Gaussians, sigma 0.15, seed
+    0; k=100, buckets <= 256, 2 Lloyd iterations, 8 repetitions + 1 pass):
+    BF16 tensor-core bucket estimates + FP32 re-rank of each point's 128 best
+    candidates, against the plain FP32 form at the same repetition count.
+    Recall over all points against FP64 brute force; the error of the returned
+    distances and of the BF16 estimates (on 16 groups of 128 nearest
+    neighbours, centred on the group's first point as a bucket is) against
+    FP64; device time per build (CUDA events on the library's stream)."""
+    import torch
+
+    from sigmod23ann_b200 import KnngContext, Stats, default_params, groundtruth, workloads
+    from sigmod23ann_b200.api import PRECISION_BF16_RERANK, PRECISION_FP32, debug_tile_gram_bf16
+
+    pts = workloads.gaussian_mixture(n=100_000, d=100, clusters=64, sigma=0.15, seed=0)
+    n = len(pts)
+    x = torch.from_numpy(pts).to(f"cuda:{device}")
+    gt = np.concatenate([groundtruth.exact_knn_torch(x, np.arange(a, min(n, a + 8192)), K)
+                         for a in range(0, n, 8192)])
+    out = {}
+    with KnngContext(device) as ctx:
+        for name, prec in (("fp32", PRECISION_FP32), ("bf16_rerank", PRECISION_BF16_RERANK)):
+            params = default_params(k=K, max_leaf=257, max_leaf_odd=0, lloyd_iters=2, reps=8, refine=1, seed=SEED,
+                                    precision=prec)
+            ids = torch.empty((n, K), dtype=torch.int32, device=x.device)
+            dist = torch.empty((n, K), dtype=torch.float32, device=x.device)
+            ctx.build_device(x.data_ptr(), n, DIM, ids.data_ptr(), dist.data_ptr(), params)
+            times = []
+            for _ in range(steps):
+                st = Stats()
+                ctx.build_device(x.data_ptr(), n, DIM, ids.data_ptr(), dist.data_ptr(), params, stats=st)
+                times.append(st.ms_total + st.ms_finalize)
+            ids_np = ids.cpu().numpy().view(np.uint32).astype(np.int64)
+            rec = groundtruth.recall(ids_np, gt, np.arange(n))
+            # returned distances against FP64 (sampled rows, every neighbour)
+            rows = np.random.default_rng(1).choice(n, 2000, replace=False)
+            xr = x[torch.as_tensor(rows, device=x.device)].double()
+            xn = x[torch.as_tensor(ids_np[rows].reshape(-1), device=x.device)].double().reshape(len(rows), K, DIM)
+            exact = ((xn - xr[:, None, :]) ** 2).sum(-1)
+            got = dist[torch.as_tensor(rows, device=x.device)].double()
+            rel = ((got - exact).abs() / exact.clamp_min(1e-30)).cpu().numpy()
+            out[name] = {"recall": rec, "ms_per_build": float(np.mean(times)),
+                         "points_per_s": n / (np.mean(times) / 1000.0),
+                         "dist_rel_err_max": float(rel.max()), "dist_rel_err_mean": float(rel.mean())}
+        # BF16 estimates on bucket-like groups (a point and its 127 nearest)
+        errs = []
+        for g in np.random.default_rng(2).choice(n, 16, replace=False):
+            grp = np.concatenate([[g], gt[g][:127]])
+            rows32 = pts[grp].astype(np.float32)
+            cen = (rows32 - rows32[0]).astype(np.float32)
+            gram = debug_tile_gram_bf16(ctx, cen, cen).astype(np.float64)
+            nrm = (cen.astype(np.float64) ** 2).sum(1)
+            est = nrm[:, None] + nrm[None, :] - 2.0 * gram
+            ex = ((rows32[:, None, :].astype(np.float64) - rows32[None, :, :]) ** 2).sum(-1)
+            mask = ~np.eye(len(grp), dtype=bool)
+            errs.append(np.abs(est - ex)[mask] / ex[mask])
+        e = np.concatenate(errs)
+        out["bf16_estimate_rel_err_max"] = float(e.max())
+        out["bf16_estimate_rel_err_mean"] = float(e.mean())
+    out["recall_change"] = out["bf16_rerank"]["recall"] - out["fp32"]["recall"]
+    out["speedup"] = out["fp32"]["ms_per_build"] / out["bf16_rerank"]["ms_per_build"]
+    out["workload"] = ("100,000 x 100 f32, 64 Gaussians (sigma 0.15, seed 0), k=100, buckets <= 256, 2 Lloyd "
+                       "iterations, 8 repetitions + 1 neighbour-of-neighbour pass; recall over all points vs FP64")
+    return out
+
+
 # ------------------------------------------------------------ batched arm
 
 def batched_sets(seed: int = 2, count: int = 4096):
@@ -577,6 +647,12 @@ def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.precision:
+        res = run_precision()
+        print(json.dumps({"metric": "precision form: recall change and speed vs the FP32 form (100k config)",
+                          "value": res["bf16_rerank"]["points_per_s"], "unit": "points/s", "higher_is_better": True,
+                          "n_gpus": 1, "dtype": "bf16 estimates + f32 re-rank", "precision": res}))
+        return 0
     if args.batched:
         res = run_batched(args.batched_waves)
         print(json.dumps({"metric": "points/sec, batched k-NN graph builds (4,096 sets)", "value": res["points_per_s"],

@@ -52,7 +52,9 @@ typedef enum knng_status {
 
 enum {
     KNNG_PRECISION_FP32 = 0,       /* exact FP32 distances everywhere (bit-exact form) */
-    KNNG_PRECISION_BF16_RERANK = 1 /* reserved: BF16 tensor-core distances + FP32 re-rank */
+    KNNG_PRECISION_BF16_RERANK = 1 /* bucket distances estimated in BF16 on the tensor cores (FP32
+                                      accumulation, FP32 norms), each point's 128 best candidates
+                                      re-ranked with exact FP32 distances; buckets <= 512 points */
 };
 
 /* Build parameters.  knng_default_params() fills the reference's values. */
@@ -213,6 +215,12 @@ knng_status knng_finalize(knng_context* ctx, uint32_t* out_ids, float* out_dists
  * with TF32 operands and FP32 accumulation. */
 knng_status knng_debug_tile_gram(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n,
                                  uint32_t d, float* out);
+
+/* The same with BF16 operands (tcgen05.mma kind::f16, FP32 accumulation): the
+ * tile the precision form estimates bucket distances with.  No counterpart in
+ * the reference. */
+knng_status knng_debug_tile_gram_bf16(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n,
+                                      uint32_t d, float* out);
 
 /* ------------------------------------------------------ allocation-free pass
  * No counterpart in the reference.  For callers that cannot allocate device

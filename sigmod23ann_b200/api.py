@@ -35,7 +35,7 @@ EXPORTED = [
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
-    "knng_debug_tile_gram", "knng_refine_pointwise_noalloc", "knng_build_batch",
+    "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_refine_pointwise_noalloc", "knng_build_batch",
     "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
     "knng_server_job_error", "knng_server_release", "knng_server_destroy",
 ]
@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH):
         "knng_set_sets": (c_int, [P, P, P, P, P, P]),
         "knng_finalize": (c_int, [P, P, P]),
         "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
+        "knng_debug_tile_gram_bf16": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_refine_pointwise_noalloc": (c_int, [P, c_uint32, c_uint32, c_uint32, P, P, P, P, P, P, P, P]),
         "knng_build_batch": (c_int, [P, P, c_uint32, c_uint32, c_uint64, P, c_uint32, c_int, POINTER(Params), P, P,
                                      POINTER(Stats)]),
@@ -357,6 +358,16 @@ def debug_tile_gram(ctx: "KnngContext", a: np.ndarray, b: np.ndarray) -> np.ndar
     b = _f32(b)
     out = np.zeros((a.shape[0], b.shape[0]), np.float32)
     ctx._check(ctx._lib.knng_debug_tile_gram(ctx._h, _ptr(a), a.shape[0], _ptr(b), b.shape[0], a.shape[1], _ptr(out)))
+    return out
+
+
+def debug_tile_gram_bf16(ctx: "KnngContext", a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """a . b^T through one tcgen05 BF16 tile, FP32 accumulation (diagnostic)."""
+    a = _f32(a)
+    b = _f32(b)
+    out = np.zeros((a.shape[0], b.shape[0]), np.float32)
+    ctx._check(ctx._lib.knng_debug_tile_gram_bf16(ctx._h, _ptr(a), a.shape[0], _ptr(b), b.shape[0], a.shape[1],
+                                                  _ptr(out)))
     return out
 
 

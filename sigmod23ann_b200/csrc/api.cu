@@ -361,7 +361,7 @@ std::vector<uint32_t> split_level(Context& c, const std::vector<Node>& active, u
 }
 
 void run_rep(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold, uint64_t seed,
-             uint32_t rep, RepStats& st, knng_stats* stats) {
+             uint32_t rep, RepStats& st, knng_stats* stats, uint32_t precision = KNNG_PRECISION_FP32) {
     require_sets(c);
     if (max_leaf < 2) fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be >= 2");
     EventPair split_t(c);
@@ -405,7 +405,10 @@ void run_rep(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small
     const uint32_t nl = static_cast<uint32_t>(leaves.size());
     uint32_t* d_ls = upload(c, "leaf_start", c.last_leaf_start.data(), nl);
     uint32_t* d_le = upload(c, "leaf_end", c.last_leaf_end.data(), nl);
-    launch_leaves(c, nl, d_ls, d_le, max_bucket, nullptr);
+    if (precision == KNNG_PRECISION_BF16_RERANK)
+        launch_leaves_bf16(c, nl, d_ls, d_le, max_bucket);
+    else
+        launch_leaves(c, nl, d_ls, d_le, max_bucket, nullptr);
     const double leaf_ms = leaf_t.stop(c);
     st.ms_leaf += leaf_ms;
     if (stats) {
@@ -450,7 +453,10 @@ void validate_params(const knng_params* p) {
     if (p->max_leaf < 2 || (p->max_leaf_odd != 0 && p->max_leaf_odd < 2))
         fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be >= 2");
     if (p->max_leaf > 4097 || p->max_leaf_odd > 4097) fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be <= 4097");
-    if (p->precision != KNNG_PRECISION_FP32) fail(KNNG_ERR_UNSUPPORTED, "only KNNG_PRECISION_FP32 is built");
+    if (p->precision != KNNG_PRECISION_FP32 && p->precision != KNNG_PRECISION_BF16_RERANK)
+        fail(KNNG_ERR_UNSUPPORTED, "unknown precision");
+    if (p->precision == KNNG_PRECISION_BF16_RERANK && (p->max_leaf > 513 || p->max_leaf_odd > 513))
+        fail(KNNG_ERR_UNSUPPORTED, "the BF16 form takes buckets of at most 512 points (max_leaf <= 513)");
 }
 
 void build_all(Context& c, const knng_params* p, knng_stats* stats) {
@@ -460,7 +466,7 @@ void build_all(Context& c, const knng_params* p, knng_stats* stats) {
     for (uint32_t r = 0; r < p->reps; ++r) {
         const uint32_t leaf = (p->max_leaf_odd != 0 && (r % 2 == 1)) ? p->max_leaf_odd : p->max_leaf;
         RepStats st;
-        run_rep(c, leaf, p->lloyd_iters, p->small_threshold, p->seed, r, st, stats);
+        run_rep(c, leaf, p->lloyd_iters, p->small_threshold, p->seed, r, st, stats, p->precision);
         add_rep_stats(stats, st);
         if (stats) stats->reps_done += 1;
     }
@@ -888,6 +894,20 @@ knng_status knng_build_device(knng_context* ctx, const float* d_points, uint32_t
             stats->kernel_launches += c.launches - l0;
         }
         KNNG_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+knng_status knng_debug_tile_gram_bf16(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n,
+                                      uint32_t d, float* out) {
+    return knng::guarded(ctx, [&](Context& c) {
+        if (!a || !b || !out) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null array");
+        if (m == 0 || n == 0 || m > 128 || n > 128) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "m and n must be in 1..128");
+        if (!knng::dim_supported(d)) knng::fail(KNNG_ERR_UNSUPPORTED, "dimension must be 64, 100 or 128");
+        float* da = knng::upload(c, "dbg_a", a, static_cast<size_t>(m) * d);
+        float* db = knng::upload(c, "dbg_b", b, static_cast<size_t>(n) * d);
+        float* dout = static_cast<float*>(knng::scratch(c, "dbg_out", static_cast<size_t>(m) * n * sizeof(float)));
+        knng::run_tile_gram_bf16(c, d, da, m, db, n, dout);
+        knng::download(c, out, dout, static_cast<size_t>(m) * n);
     });
 }
 

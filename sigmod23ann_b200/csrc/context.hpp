@@ -156,6 +156,13 @@ void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, cons
 // leaf.cu
 void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
                    uint32_t max_bucket, uint64_t* evals);
+// leaf_bf16.cu: the precision form (BF16 tensor-core estimates, the 128 best
+// candidates per point re-ranked in FP32), buckets of at most 512 points.
+void launch_leaves_bf16(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
+                        uint32_t max_bucket);
+// One 128 x 128 BF16 tile a(m x d) . b(n x d)^T into d_out (m x n), m, n <= 128.
+void run_tile_gram_bf16(Context& c, uint32_t d, const float* d_a, uint32_t m, const float* d_b, uint32_t n,
+                        float* d_out);
 // refine.cu
 uint64_t run_refine(Context& c);
 // One tensor-core tile a(m x d) . b(n x d)^T into d_out (m x n), m, n <= 128.

@@ -170,6 +170,41 @@ __device__ __forceinline__ void issue_tile_tf32(uint32_t tmem_d, uint32_t a_base
     }
 }
 
+// Instruction descriptor: kind::f16 with BF16 A and B, F32 accumulate, both
+// K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N) {
+    return (1u << 4)                // D format: F32
+           | (1u << 7)              // A format: BF16
+           | (1u << 10)             // B format: BF16
+           | ((N >> 3) << 17)       // N / 8
+           | ((M >> 4) << 24);      // M / 16
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t desc_a, uint64_t desc_b, uint32_t idesc,
+                                         bool accumulate) {
+    const uint32_t acc = accumulate ? 1u : 0u;
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        :
+        : "r"(tmem_d), "l"(desc_a), "l"(desc_b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+
+// Issues the K/16 MMAs of one 128 x N BF16 tile (call from a single thread).
+// The operand tiles use the same chunk-major layout as the TF32 ones, a
+// 16-byte chunk holding 8 BF16 values; one MMA consumes K = 16 (two chunks).
+__device__ __forceinline__ void issue_tile_bf16(uint32_t tmem_d, uint32_t a_base, uint32_t b_base, uint32_t a_rows,
+                                                uint32_t b_rows, uint32_t kpad, uint32_t idesc) {
+    for (uint32_t s = 0; s < kpad / 16; ++s) {
+        const uint64_t da = smem_desc(a_base + 2 * s * a_rows * 16, a_rows * 16, 128);
+        const uint64_t db = smem_desc(b_base + 2 * s * b_rows * 16, b_rows * 16, 128);
+        mma_bf16(tmem_d, da, db, idesc, s > 0);
+    }
+}
+
 // Byte offset of element (row r, k) in a chunk-major tile with `rows` rows.
 __host__ __device__ constexpr uint32_t chunk_offset(uint32_t r, uint32_t k, uint32_t rows) {
     return (k >> 2) * rows * 16 + r * 16 + (k & 3) * 4;

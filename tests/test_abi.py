@@ -18,7 +18,7 @@ def declared_symbols() -> list[str]:
     for h in ("knng.h",):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        names += re.findall(r"\b(knng_[a-z_]+)\s*\(", text)
+        names += re.findall(r"\b(knng_[a-z0-9_]+)\s*\(", text)
     return sorted(set(names))
 
 
