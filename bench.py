@@ -66,6 +66,9 @@ def parse_args(argv=None):
                     help="requests of the serving stream measured beside the build (0: skip)")
     ap.add_argument("--serving", action="store_true", help="measure only the serving stream")
     ap.add_argument("--batched", action="store_true", help="measure only the batched form (4,096 sets, 5 waves)")
+    ap.add_argument("--bf16", action="store_true",
+                    help="time the precision form (BF16 estimates + FP32 re-rank, buckets <= 512) instead")
+    ap.add_argument("--max-leaf", type=int, default=0, help="leaf test bound (0: 1025, or 513 with --bf16)")
     ap.add_argument("--precision", action="store_true",
                     help="measure only the precision form against the FP32 form (100k-point config)")
     ap.add_argument("--batched-waves", type=int, default=5, help="waves of the batched form to run (of 5)")
@@ -502,8 +505,12 @@ def run_ours(args):
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     n = args.n
-    params = default_params(k=K, max_leaf=MAX_LEAF, max_leaf_odd=0, lloyd_iters=LLOYD_ITERS, reps=args.reps,
-                            refine=args.refine, seed=SEED)
+    from sigmod23ann_b200.api import PRECISION_BF16_RERANK, PRECISION_FP32
+
+    max_leaf = args.max_leaf or (513 if args.bf16 else MAX_LEAF)
+    params = default_params(k=K, max_leaf=max_leaf, max_leaf_odd=0, lloyd_iters=LLOYD_ITERS, reps=args.reps,
+                            refine=args.refine, seed=SEED,
+                            precision=PRECISION_BF16_RERANK if args.bf16 else PRECISION_FP32)
     x = workloads.subspace_mixture_torch(n, seed=SEED, device=f"cuda:{local}")
     ids = torch.empty((n, K), dtype=torch.int32, device=f"cuda:{local}")
     ctx = KnngContext(local)
@@ -609,9 +616,10 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{n:,} x {DIM} f32, 1024-cluster Zipf(1.1) 24-d subspace mixture (seed {SEED}), "
-                                   f"k={K}, leaf<=1024, {args.reps} repetitions, {LLOYD_ITERS} Lloyd iterations, "
-                                   f"{args.refine} neighbour-of-neighbour passes",
-                       "n": n, "k": K, "reps": args.reps, "parallelism": f"replicas x{world}",
+                                   f"k={K}, leaf<={max_leaf - 1}, {args.reps} repetitions, {LLOYD_ITERS} Lloyd "
+                                   f"iterations, {args.refine} neighbour-of-neighbour passes"
+                                   + (", BF16 bucket estimates + FP32 re-rank" if args.bf16 else ", FP32"),
+                       "n": n, "k": K, "reps": args.reps, "precision": "bf16_rerank" if args.bf16 else "fp32", "parallelism": f"replicas x{world}",
                        "l2": "input 4 GB > 126 MB L2; no flush between steps"},
             "recall": rec, "recall_queries": len(q), "meets_recall_target": rec >= 0.94,
             "clocks": clock, "gpu_launches": launches, "stream_ms_total": stream_ms, "wall_s": wall,
