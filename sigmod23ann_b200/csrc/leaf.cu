@@ -94,7 +94,7 @@ __device__ __forceinline__ void distance_block(const float* __restrict__ I, cons
 }
 
 template <int D>
-__global__ void __launch_bounds__(kLeafThreads, 1)
+__global__ void __launch_bounds__(kLeafThreads, 2)
     k_leaf(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends, const uint32_t* __restrict__ idx,
            const float* __restrict__ pts, int ld, float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
            uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound,
