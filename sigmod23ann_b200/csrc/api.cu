@@ -83,6 +83,34 @@ void* scratch(Context& c, const char* name, size_t bytes) {
     return b.ptr;
 }
 
+void* staging_take(Context& c, size_t bytes) {
+    bytes = (bytes + 15) / 16 * 16;
+    if (bytes > c.staging_cap) {
+        KNNG_CUDA(cudaStreamSynchronize(c.stream));
+        staging_free(c);
+        const size_t cap = std::max<size_t>(bytes, 4u << 20);
+        void* p = nullptr;
+        check_cuda(cudaMallocHost(&p, cap), "cudaMallocHost");
+        c.staging = static_cast<unsigned char*>(p);
+        c.staging_cap = cap;
+        c.staging_used = 0;
+    }
+    if (c.staging_used + bytes > c.staging_cap) {
+        // Every copy through the space must land before it is reused.
+        KNNG_CUDA(cudaStreamSynchronize(c.stream));
+        c.staging_used = 0;
+    }
+    void* p = c.staging + c.staging_used;
+    c.staging_used += bytes;
+    return p;
+}
+
+void staging_free(Context& c) {
+    if (c.staging) cudaFreeHost(c.staging);
+    c.staging = nullptr;
+    c.staging_cap = c.staging_used = 0;
+}
+
 size_t scratch_bytes(const Context& c, const char* name) {
     for (const auto& e : c.scratch)
         if (e.first == name) return e.second.bytes;
@@ -571,6 +599,7 @@ knng_status knng_destroy(knng_context* ctx) {
     if (!c) return KNNG_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     knng::release_all(*c);
+    knng::staging_free(*c);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return KNNG_OK;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -70,6 +71,12 @@ struct Context {
 
     uint64_t launches = 0;
 
+    // Pinned host staging for small transfers: an upload is copied here and
+    // sent asynchronously, a download lands here first; the space is reused
+    // after the next synchronisation of the stream.
+    unsigned char* staging = nullptr;
+    size_t staging_cap = 0, staging_used = 0;
+
     // Neighbour-of-neighbour pass: 0 = local join on the tensor cores,
     // 1 = one warp per point (environment KNNG_REFINE=pointwise at creation).
     int refine_mode = 0;
@@ -94,18 +101,42 @@ void* scratch(Context& c, const char* name, size_t bytes);
 size_t scratch_bytes(const Context& c, const char* name);
 void release_all(Context& c);
 
+// Transfers up to this size go through the pinned staging space.
+constexpr size_t kStagedMax = 1u << 20;
+// `bytes` of pinned staging space (synchronises the stream and starts over
+// when the space is used up; grows it when one transfer needs more).
+void* staging_take(Context& c, size_t bytes);
+void staging_free(Context& c);
+
 // Uploads `count` elements into named scratch and returns the device pointer.
 template <class T>
 T* upload(Context& c, const char* name, const T* host, size_t count) {
     T* d = static_cast<T*>(scratch(c, name, count * sizeof(T) + 16));
-    if (count) KNNG_CUDA(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    const size_t bytes = count * sizeof(T);
+    if (bytes == 0) return d;
+    if (bytes <= kStagedMax) {
+        void* p = staging_take(c, bytes);
+        std::memcpy(p, host, bytes);
+        KNNG_CUDA(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, c.stream));
+    } else {
+        KNNG_CUDA(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, c.stream));
+    }
     return d;
 }
 
 template <class T>
 void download(Context& c, T* host, const T* dev, size_t count) {
-    if (count) KNNG_CUDA(cudaMemcpyAsync(host, dev, count * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
-    KNNG_CUDA(cudaStreamSynchronize(c.stream));
+    const size_t bytes = count * sizeof(T);
+    if (bytes > 0 && bytes <= kStagedMax) {
+        void* p = staging_take(c, bytes);
+        KNNG_CUDA(cudaMemcpyAsync(p, dev, bytes, cudaMemcpyDeviceToHost, c.stream));
+        KNNG_CUDA(cudaStreamSynchronize(c.stream));
+        std::memcpy(host, p, bytes);
+    } else {
+        if (bytes) KNNG_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c.stream));
+        KNNG_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    c.staging_used = 0;  // every earlier copy through the staging space has completed
 }
 
 bool dim_supported(uint32_t d);
