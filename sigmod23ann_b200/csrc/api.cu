@@ -219,7 +219,9 @@ void load_points(Context& c, const float* pts, uint32_t n, uint32_t d, uint64_t 
     if (ld_bytes == 0) ld_bytes = static_cast<uint64_t>(d) * sizeof(float);
     if (ld_bytes < static_cast<uint64_t>(d) * sizeof(float) || ld_bytes % sizeof(float) != 0)
         fail(KNNG_ERR_INVALID_ARGUMENT, "ld_bytes must be a multiple of 4 and >= 4*d");
-    const bool same_shape = c.points && c.n == n && c.d == d && !c.points_borrowed;
+    // Same shape: keep the sets, order and scratch (only the points change,
+    // whether they are copied in or borrowed).
+    const bool same_shape = c.indices && c.n == n && c.d == d;
     if (!same_shape) {
         const uint32_t k = c.k;
         const bool had_sets = c.set_dist != nullptr;

@@ -285,6 +285,14 @@ knng_status knng_server_destroy(knng_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& t : s->workers) t.join();
+    // Hand the memory the jobs cached in the device's default pool back.
+    cudaSetDevice(s->device);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+        uint64_t keep = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        cudaMemPoolTrimTo(pool, 0);
+    }
     delete s;
     return KNNG_OK;
 }
