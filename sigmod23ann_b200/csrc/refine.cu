@@ -2,18 +2,31 @@
 // (src/SolutionKmeans.hpp:480-555).
 //
 // Snapshot: every set's k slot ids, sorted ascending, unfilled slots included
-// as id 0 -- the reference reads all 100 current_ids (:494).  Then, per point
-// p, the candidates are the union of the snapshot lists of p's snapshot list,
-// minus p, each offered with the exact distance when dist < bound.
+// (as the point set's first id, 0 for a single set) -- the reference reads all
+// 100 current_ids (:494).  Per point p, the candidates are the union of the
+// snapshot lists of p's snapshot list, minus p, each offered with the exact
+// distance when dist < bound.
 //
 // The reference iterates its candidate set in hash order; this pass offers
 // them in ascending id order.  The order can only matter between candidates
-// that beat the bound p had when its pass started, so each warp evaluates all
-// candidates (one lane per candidate, row gathered from HBM/L2), keeps the
-// survivors (dist < starting bound), sorts them by id and replays them in that
-// order through the sequential set update.  Survivors are staged in a
-// per-warp scratch region of k*k entries (rounded up to a power of two) and
-// sorted in shared memory when they fit.
+// that beat the bound p had when its pass started, so the pass collects every
+// such survivor (dist < starting bound), sorts each point's survivors by id and
+// replays them in that order through the sequential set update.
+//
+// Two ways to collect the survivors, with the same result:
+//   * the local join (k_join, the default): per point q, the rows R(q) (points
+//     whose list holds q) against the columns S(q) (q's list) as one block; a
+//     tcgen05 TF32 tile of centred dot products rejects the pairs that provably
+//     cannot beat bound(p), members of S(p) are dropped, the rest get the exact
+//     FP32 distance; survivors go to per-point slots, then to the CTA's pool
+//     region (k_excess_counts / k_pool_scatter turn the pool into per-point
+//     lists), and one k_apply launch sorts and replays every point's survivors;
+//   * one warp per point (k_refine): the warp walks its candidates (one lane per
+//     candidate, rows gathered from HBM/L2) with a shared-memory seen-set, keeps
+//     the survivors in shared memory (or a per-warp global region of k*k
+//     entries) and replays them.  It serves as the cross-check of the join
+//     (environment KNNG_REFINE=pointwise), as the pass for the points whose
+//     pool region filled up, and behind the allocation-free entry point.
 #include <cuda_runtime.h>
 
 #include <algorithm>
