@@ -244,9 +244,11 @@ void load_points(Context& c, const float* pts, uint32_t n, uint32_t d, uint64_t 
             c.points = static_cast<float*>(dev_alloc(c, static_cast<size_t>(n) * row));
             c.points_borrowed = false;
         }
-        if (n > 0)
-            KNNG_CUDA(cudaMemcpy2DAsync(c.points, row, pts, ld_bytes, row, n,
-                                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+        const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if (n > 0 && ld_bytes == row)  // packed rows: one contiguous copy
+            KNNG_CUDA(cudaMemcpyAsync(c.points, pts, static_cast<size_t>(n) * row, kind, c.stream));
+        else if (n > 0)
+            KNNG_CUDA(cudaMemcpy2DAsync(c.points, row, pts, ld_bytes, row, n, kind, c.stream));
     }
     c.set_offsets = {0u, n};
     c.d_set_offsets = nullptr;
