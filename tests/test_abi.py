@@ -119,3 +119,23 @@ def test_server_without_device_reports_no_device(knng_lib):
     with pytest.raises(api.KnngError) as e:
         api.KnngServer(0)
     assert e.value.status == 7
+
+
+def test_null_handles_are_refused(knng_lib):
+    """Entry points given a null context or server answer
+    KNNG_ERR_INVALID_ARGUMENT without touching a device."""
+    from sigmod23ann_b200.api import JobInfo, Params
+
+    p = Params()
+    knng_lib.knng_default_params(ctypes.byref(p))
+    job = ctypes.c_uint64()
+    info = JobInfo()
+    assert knng_lib.knng_server_submit(None, None, 10, 100, 400, ctypes.byref(p), None, None, ctypes.byref(job)) == 1
+    assert knng_lib.knng_server_poll(None, 1, ctypes.byref(info)) == 1
+    assert knng_lib.knng_server_wait(None, 1, 0, ctypes.byref(info)) == 1
+    assert knng_lib.knng_server_release(None, 1) == 1
+    assert knng_lib.knng_server_destroy(None) == 1
+    assert knng_lib.knng_server_job_error(None, 1) == b"null server"
+    assert knng_lib.knng_build_batch(None, None, 10, 100, 400, None, 1, 0, ctypes.byref(p), None, None, None) == 1
+    out = ctypes.c_void_p()
+    assert knng_lib.knng_server_create(0, 0, 0, ctypes.byref(out)) == 1  # max_running must be >= 1
