@@ -250,6 +250,18 @@ knng_status knng_refine_pointwise_noalloc(const float* d_points, uint32_t n, uin
                                           uint32_t* d_snapshot, float* d_dist, uint32_t* d_ids, uint32_t* d_size,
                                           uint32_t* d_maxslot, float* d_bound, uint32_t* d_changed, void* stream);
 
+/* SolutionKmeans::constructResult's wall-clock schedule
+ * (src/SolutionKmeans.hpp:579-604): knng_build with time budgets instead of
+ * fixed counts.  Repetitions (alternating max_leaf / max_leaf_odd) run while
+ * less than build_ms has passed since the call began -- at least one, at most
+ * params->reps when it is non-zero; then whole refinement passes start while
+ * less than build_ms + refine_ms has passed, at most params->refine (the
+ * reference cuts its single pass short instead).  stats->reps_done tells how
+ * many repetitions ran.  Host pointers. */
+knng_status knng_build_timed(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                             const knng_params* params, uint64_t build_ms, uint64_t refine_ms, uint32_t* out_ids,
+                             float* out_dists, knng_stats* stats);
+
 /* Batched form: many independent point sets in one build.  No counterpart in
  * the reference (one constructResult per process); each set is built as
  * knng_build would build it alone, with the same parameters and result, but

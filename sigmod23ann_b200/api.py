@@ -36,7 +36,7 @@ EXPORTED = [
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
     "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_refine_pointwise_noalloc", "knng_build_batch",
-    "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
+    "knng_build_timed", "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
     "knng_server_job_error", "knng_server_release", "knng_server_destroy",
 ]
 
@@ -119,6 +119,8 @@ def load_library(path: str = LIB_PATH):
         "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_debug_tile_gram_bf16": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_refine_pointwise_noalloc": (c_int, [P, c_uint32, c_uint32, c_uint32, P, P, P, P, P, P, P, P]),
+        "knng_build_timed": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), c_uint64, c_uint64, P, P,
+                                     POINTER(Stats)]),
         "knng_build_batch": (c_int, [P, P, c_uint32, c_uint32, c_uint64, P, c_uint32, c_int, POINTER(Params), P, P,
                                      POINTER(Stats)]),
         "knng_job_reservation": (c_uint64, [c_uint32, c_uint32, c_uint32]),
@@ -218,6 +220,21 @@ class KnngContext:
         st = stats if stats is not None else Stats()
         self._check(self._lib.knng_build(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p), _ptr(ids),
                                          _ptr(dists), ctypes.byref(st)))
+        self.n, self.d, self.k = n, d, p.k
+        return (ids, dists) if want_dists else ids
+
+    def build_timed(self, points: np.ndarray, build_ms: int, refine_ms: int, params: Params | None = None,
+                    want_dists: bool = False, stats: Stats | None = None):
+        """knng_build_timed: repetitions while build_ms has not passed, then
+        refinement passes while build_ms + refine_ms has not."""
+        pts = _f32(points)
+        n, d = pts.shape
+        p = params or default_params()
+        ids = np.empty((n, p.k), np.uint32)
+        dists = np.empty((n, p.k), np.float32) if want_dists else None
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_build_timed(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p), build_ms,
+                                               refine_ms, _ptr(ids), _ptr(dists), ctypes.byref(st)))
         self.n, self.d, self.k = n, d, p.k
         return (ids, dists) if want_dists else ids
 

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
@@ -491,11 +492,25 @@ void validate_params(const knng_params* p) {
         fail(KNNG_ERR_UNSUPPORTED, "the BF16 form takes buckets of at most 512 points (max_leaf <= 513)");
 }
 
-void build_all(Context& c, const knng_params* p, knng_stats* stats) {
+// All repetitions, then all refinement passes.  With build_ms > 0 (the
+// reference's wall-clock loop, SolutionKmeans::constructResult,
+// src/SolutionKmeans.hpp:579-604): repetitions run while less than build_ms
+// has passed since the call began (at least one, at most p->reps when it is
+// non-zero), then whole refinement passes start while less than
+// build_ms + refine_ms has passed (at most p->refine).
+void build_all(Context& c, const knng_params* p, knng_stats* stats, uint64_t build_ms = 0, uint64_t refine_ms = 0) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto elapsed_ms = [&] {
+        KNNG_CUDA(cudaStreamSynchronize(c.stream));
+        return static_cast<uint64_t>(
+            std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count());
+    };
+    const bool timed = build_ms > 0;
     alloc_sets(c, p->k);
     EventPair total_t(c);
     const uint64_t launches0 = c.launches;
-    for (uint32_t r = 0; r < p->reps; ++r) {
+    for (uint32_t r = 0; timed ? (r == 0 || ((p->reps == 0 || r < p->reps) && elapsed_ms() < build_ms)) : r < p->reps;
+         ++r) {
         const uint32_t leaf = (p->max_leaf_odd != 0 && (r % 2 == 1)) ? p->max_leaf_odd : p->max_leaf;
         RepStats st;
         run_rep(c, leaf, p->lloyd_iters, p->small_threshold, p->seed, r, st, stats, p->precision);
@@ -503,6 +518,7 @@ void build_all(Context& c, const knng_params* p, knng_stats* stats) {
         if (stats) stats->reps_done += 1;
     }
     for (uint32_t pass = 0; pass < p->refine; ++pass) {
+        if (timed && elapsed_ms() >= build_ms + refine_ms) break;
         EventPair rt(c);
         const uint64_t ch = run_refine(c);
         add_refine_stats(stats, c, ch, rt.stop(c));
@@ -863,6 +879,27 @@ knng_status knng_build(knng_context* ctx, const float* points, uint32_t n, uint3
         if (stats) std::memset(stats, 0, sizeof(*stats));
         knng::load_points(c, points, n, d, ld_bytes, false, false);
         knng::build_all(c, params, stats);
+        const size_t nk = static_cast<size_t>(c.n) * c.k;
+        knng::EventPair ft(c);
+        uint32_t* d_ids = static_cast<uint32_t*>(knng::scratch(c, "fin_ids", nk * sizeof(uint32_t)));
+        float* d_dist = out_dists ? static_cast<float*>(knng::scratch(c, "fin_dist", nk * sizeof(float))) : nullptr;
+        knng::launch_finalize(c, d_ids, d_dist);
+        if (stats) stats->ms_finalize += ft.stop(c);
+        knng::download(c, out_ids, d_ids, nk);
+        if (out_dists) knng::download(c, out_dists, d_dist, nk);
+    });
+}
+
+knng_status knng_build_timed(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                             const knng_params* params, uint64_t build_ms, uint64_t refine_ms, uint32_t* out_ids,
+                             float* out_dists, knng_stats* stats) {
+    return knng::guarded(ctx, [&](Context& c) {
+        knng::validate_params(params);
+        if (!out_ids) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null output");
+        if (build_ms == 0) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "build_ms must be positive");
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        knng::load_points(c, points, n, d, ld_bytes, false, false);
+        knng::build_all(c, params, stats, build_ms, refine_ms);
         const size_t nk = static_cast<size_t>(c.n) * c.k;
         knng::EventPair ft(c);
         uint32_t* d_ids = static_cast<uint32_t*>(knng::scratch(c, "fin_ids", nk * sizeof(uint32_t)));

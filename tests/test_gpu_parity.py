@@ -315,3 +315,24 @@ def test_batched_build_equals_builds_alone(knng_lib):
             ids, dist = ctx.build(pts, params, want_dists=True)
         assert np.array_equal(b_ids[s], ids), f"set {s} ids"
         assert np.array_equal(b_d[s].view(np.uint32), dist.view(np.uint32)), f"set {s} distances"
+
+
+def test_timed_build_equals_fixed_count_build(knng_lib):
+    """knng_build_timed (the reference's wall-clock schedule: repetitions with
+    alternating bucket bounds while the budget lasts, then passes) builds the
+    same graph as knng_build with the repetition and pass counts it reached;
+    a budget of 1 ms still runs one repetition."""
+    from sigmod23ann_b200.api import Stats
+
+    pts = workloads.gaussian_mixture(n=20_000, d=100, clusters=16, sigma=0.15, seed=4)
+    params = default_params(reps=0, refine=1, max_leaf=200, max_leaf_odd=400, lloyd_iters=1, seed=3)
+    st = Stats()
+    with KnngContext(0) as ctx:
+        ids = ctx.build_timed(pts, build_ms=400, refine_ms=2000, params=params, stats=st)
+        assert st.reps_done >= 1
+        fixed = ctx.build(pts, default_params(reps=int(st.reps_done), refine=int(st.refine_join_launches),
+                                              max_leaf=200, max_leaf_odd=400, lloyd_iters=1, seed=3))
+        assert np.array_equal(ids, fixed)
+        one = Stats()
+        ctx.build_timed(pts, build_ms=1, refine_ms=0, params=params, stats=one)
+        assert one.reps_done == 1 and one.refine_join_launches == 0
