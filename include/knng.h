@@ -204,6 +204,15 @@ knng_status knng_get_sets(knng_context* ctx, float* dist, uint32_t* ids, uint32_
 knng_status knng_set_sets(knng_context* ctx, const float* dist, const uint32_t* ids, const uint32_t* sizes,
                           const uint32_t* maxslot, const float* bounds);
 
+/* Snapshot / resume of the neighbour sets (no counterpart in the reference):
+ * knng_save_sets writes the sets of the loaded points (distances, ids, sizes,
+ * max slots, bounds, with n and k) to a file; knng_load_sets reads such a
+ * file into a context holding the same points (same n), so that a build
+ * continues from it with further repetitions (knng_run_rep with the next
+ * rep_index), refinement passes and knng_finalize. */
+knng_status knng_save_sets(knng_context* ctx, const char* path);
+knng_status knng_load_sets(knng_context* ctx, const char* path);
+
 /* Sorted, padded output (finalize + padResult, src/KnnSets.hpp:113-126,
  * :334-344): out_ids n*k, out_dists n*k (may be NULL). Host pointers. */
 knng_status knng_finalize(knng_context* ctx, uint32_t* out_ids, float* out_dists);

@@ -36,7 +36,7 @@ EXPORTED = [
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
     "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_refine_pointwise_noalloc", "knng_build_batch",
-    "knng_build_timed", "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
+    "knng_build_timed", "knng_save_sets", "knng_load_sets", "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
     "knng_server_job_error", "knng_server_release", "knng_server_destroy",
 ]
 
@@ -119,6 +119,8 @@ def load_library(path: str = LIB_PATH):
         "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_debug_tile_gram_bf16": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_refine_pointwise_noalloc": (c_int, [P, c_uint32, c_uint32, c_uint32, P, P, P, P, P, P, P, P]),
+        "knng_save_sets": (c_int, [P, c_char_p]),
+        "knng_load_sets": (c_int, [P, c_char_p]),
         "knng_build_timed": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), c_uint64, c_uint64, P, P,
                                      POINTER(Stats)]),
         "knng_build_batch": (c_int, [P, P, c_uint32, c_uint32, c_uint64, P, c_uint32, c_int, POINTER(Params), P, P,
@@ -361,6 +363,17 @@ class KnngContext:
     def set_sets(self, s: dict) -> None:
         arrs = [_f32(s["dist"]), _u32(s["id"]), _u32(s["size"]), _u32(s["maxslot"]), _f32(s["bound"])]
         self._check(self._lib.knng_set_sets(self._h, *(_ptr(a) for a in arrs)))
+
+    def save_sets(self, path: str) -> None:
+        """Writes the neighbour sets to a file (knng_save_sets)."""
+        self._check(self._lib.knng_save_sets(self._h, os.fsencode(path)))
+
+    def load_sets(self, path: str) -> None:
+        """Reads neighbour sets saved for the same points (knng_load_sets)."""
+        self._check(self._lib.knng_load_sets(self._h, os.fsencode(path)))
+        with open(path, "rb") as f:
+            f.seek(16)
+            self.k = int(np.frombuffer(f.read(4), np.uint32)[0])
 
     def finalize(self, want_dists: bool = False):
         ids = np.zeros((self.n, self.k), np.uint32)

@@ -15,6 +15,7 @@
 #include <chrono>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -854,6 +855,76 @@ knng_status knng_set_sets(knng_context* ctx, const float* dist, const uint32_t* 
         KNNG_CUDA(cudaMemcpyAsync(c.set_size, sizes, c.n * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
         KNNG_CUDA(cudaMemcpyAsync(c.set_maxslot, maxslot, c.n * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
         KNNG_CUDA(cudaMemcpyAsync(c.set_bound, bounds, c.n * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+        KNNG_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+namespace {
+// Neighbour-set state file: "KNNGSETS", version, n, k, 0 (5 x 4 bytes after
+// the tag), then dist f32[n*k], id u32[n*k], size u32[n], max slot u32[n],
+// bound f32[n], little-endian as written by this host.
+constexpr char kSetsTag[8] = {'K', 'N', 'N', 'G', 'S', 'E', 'T', 'S'};
+constexpr uint32_t kSetsVersion = 1;
+}  // namespace
+
+knng_status knng_save_sets(knng_context* ctx, const char* path) {
+    return knng::guarded(ctx, [&](Context& c) {
+        knng::require_sets(c);
+        if (!path) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null path");
+        const size_t nk = static_cast<size_t>(c.n) * c.k;
+        std::vector<float> dist(nk), bound(c.n);
+        std::vector<uint32_t> ids(nk), size(c.n), maxslot(c.n);
+        knng::download(c, dist.data(), c.set_dist, nk);
+        knng::download(c, ids.data(), c.set_id, nk);
+        knng::download(c, size.data(), c.set_size, c.n);
+        knng::download(c, maxslot.data(), c.set_maxslot, c.n);
+        knng::download(c, bound.data(), c.set_bound, c.n);
+        std::FILE* f = std::fopen(path, "wb");
+        if (!f) knng::fail(KNNG_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
+        const uint32_t head[4] = {kSetsVersion, c.n, c.k, 0u};
+        bool ok = std::fwrite(kSetsTag, 1, 8, f) == 8 && std::fwrite(head, 4, 4, f) == 4 &&
+                  std::fwrite(dist.data(), 4, nk, f) == nk && std::fwrite(ids.data(), 4, nk, f) == nk &&
+                  std::fwrite(size.data(), 4, c.n, f) == c.n && std::fwrite(maxslot.data(), 4, c.n, f) == c.n &&
+                  std::fwrite(bound.data(), 4, c.n, f) == c.n;
+        ok = (std::fclose(f) == 0) && ok;
+        if (!ok) knng::fail(KNNG_ERR_INVALID_ARGUMENT, std::string("short write to ") + path);
+    });
+}
+
+knng_status knng_load_sets(knng_context* ctx, const char* path) {
+    return knng::guarded(ctx, [&](Context& c) {
+        knng::require_points(c);
+        if (!path) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null path");
+        std::FILE* f = std::fopen(path, "rb");
+        if (!f) knng::fail(KNNG_ERR_INVALID_ARGUMENT, std::string("cannot read ") + path);
+        char tag[8];
+        uint32_t head[4];
+        bool ok = std::fread(tag, 1, 8, f) == 8 && std::memcmp(tag, kSetsTag, 8) == 0 &&
+                  std::fread(head, 4, 4, f) == 4 && head[0] == kSetsVersion;
+        if (!ok || head[1] != c.n || head[2] == 0 || head[2] > static_cast<uint32_t>(knng::kMaxK)) {
+            std::fclose(f);
+            knng::fail(KNNG_ERR_INVALID_ARGUMENT, "not a set-state file of this point count");
+        }
+        const uint32_t k = head[2];
+        const size_t nk = static_cast<size_t>(c.n) * k;
+        std::vector<float> dist(nk), bound(c.n);
+        std::vector<uint32_t> ids(nk), size(c.n), maxslot(c.n);
+        ok = std::fread(dist.data(), 4, nk, f) == nk && std::fread(ids.data(), 4, nk, f) == nk &&
+             std::fread(size.data(), 4, c.n, f) == c.n && std::fread(maxslot.data(), 4, c.n, f) == c.n &&
+             std::fread(bound.data(), 4, c.n, f) == c.n;
+        std::fclose(f);
+        if (!ok) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "truncated set-state file");
+        for (uint32_t i = 0; i < c.n; ++i) {
+            if (size[i] > k) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "set size above k");
+            if (size[i] == k && maxslot[i] >= k) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "full set without a max slot");
+        }
+        knng::alloc_sets(c, k);
+        KNNG_CUDA(cudaMemcpyAsync(c.set_dist, dist.data(), nk * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+        KNNG_CUDA(cudaMemcpyAsync(c.set_id, ids.data(), nk * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+        KNNG_CUDA(cudaMemcpyAsync(c.set_size, size.data(), c.n * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+        KNNG_CUDA(
+            cudaMemcpyAsync(c.set_maxslot, maxslot.data(), c.n * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+        KNNG_CUDA(cudaMemcpyAsync(c.set_bound, bound.data(), c.n * sizeof(float), cudaMemcpyHostToDevice, c.stream));
         KNNG_CUDA(cudaStreamSynchronize(c.stream));
     });
 }

@@ -139,3 +139,8 @@ def test_null_handles_are_refused(knng_lib):
     assert knng_lib.knng_build_batch(None, None, 10, 100, 400, None, 1, 0, ctypes.byref(p), None, None, None) == 1
     out = ctypes.c_void_p()
     assert knng_lib.knng_server_create(0, 0, 0, ctypes.byref(out)) == 1  # max_running must be >= 1
+
+
+def test_set_state_entry_points_refuse_null(knng_lib):
+    assert knng_lib.knng_save_sets(None, b"/nonexistent") == 1
+    assert knng_lib.knng_load_sets(None, b"/nonexistent") == 1

@@ -336,3 +336,27 @@ def test_timed_build_equals_fixed_count_build(knng_lib):
         one = Stats()
         ctx.build_timed(pts, build_ms=1, refine_ms=0, params=params, stats=one)
         assert one.reps_done == 1 and one.refine_join_launches == 0
+
+
+def test_sets_snapshot_and_resume(knng_lib, tmp_path):
+    """Two repetitions, the sets saved to a file; a fresh context with the
+    same points loads them and runs repetition 2 and a pass: the graph equals
+    a straight three-repetition build."""
+    pts = workloads.gaussian_mixture(n=20_000, d=100, clusters=16, sigma=0.15, seed=8)
+    params = default_params(reps=3, refine=1, max_leaf=257, max_leaf_odd=0, lloyd_iters=2, seed=5)
+    with KnngContext(0) as ctx:
+        straight = ctx.build(pts, params)
+    path = str(tmp_path / "sets.bin")
+    with KnngContext(0) as a:
+        a.load_points(pts)
+        a.reset_sets(100)
+        for r in range(2):
+            a.run_rep(257, 2, 3000, seed=5, rep_index=r)
+        a.save_sets(path)
+    with KnngContext(0) as b:
+        b.load_points(pts)
+        b.load_sets(path)
+        b.run_rep(257, 2, 3000, seed=5, rep_index=2)
+        b.refine()
+        resumed = b.finalize()
+    assert np.array_equal(resumed, straight)
