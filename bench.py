@@ -414,6 +414,23 @@ def run_precision(device: int = 0, steps: int = 3) -> dict:
         e = np.concatenate(errs)
         out["bf16_estimate_rel_err_max"] = float(e.max())
         out["bf16_estimate_rel_err_mean"] = float(e.mean())
+    # The reference's own CPU code on the same config, in full (all host threads).
+    try:
+        from oracle import bindings
+
+        os.environ.setdefault("KNNG_REF_THREADS", str(os.cpu_count() or 1))
+        if bindings.reference_available():
+            ref = bindings.ReferenceShim(pts, threaded=True)
+            t = time.perf_counter()
+            for _ in range(8):
+                ref.rep(2, 257)
+            ref.topup()
+            dt = time.perf_counter() - t
+            ref.close()
+            out["cpu_reference"] = {"seconds": dt, "points_per_s": n / dt, "cores": int(os.environ["KNNG_REF_THREADS"]),
+                                    "kind": "reference"}
+    except Exception as e:  # the baseline must not hide the GPU figures
+        out["cpu_reference"] = {"error": str(e)}
     out["recall_change"] = out["bf16_rerank"]["recall"] - out["fp32"]["recall"]
     out["speedup"] = out["fp32"]["ms_per_build"] / out["bf16_rerank"]["ms_per_build"]
     out["workload"] = ("100,000 x 100 f32, 64 Gaussians (sigma 0.15, seed 0), k=100, buckets <= 256, 2 Lloyd "
