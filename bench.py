@@ -180,6 +180,16 @@ def dist_done(world: int):
         dist.destroy_process_group()
 
 
+def workload_config(n: int, reps: int, refine: int, max_leaf: int, bf16: bool, world: int) -> dict:
+    """The `config` object of the build line, the same for both arms."""
+    return {"workload": f"{n:,} x {DIM} f32, 1024-cluster Zipf(1.1) 24-d subspace mixture (seed {SEED}), "
+                        f"k={K}, leaf<={max_leaf - 1}, {reps} repetitions, {LLOYD_ITERS} Lloyd "
+                        f"iterations, {refine} neighbour-of-neighbour passes"
+                        + (", BF16 bucket estimates + FP32 re-rank" if bf16 else ", FP32"),
+            "n": n, "k": K, "reps": reps, "precision": "bf16_rerank" if bf16 else "fp32",
+            "parallelism": f"replicas x{world}", "l2": "input 4 GB > 126 MB L2; no flush between steps"}
+
+
 # ------------------------------------------------------------ reference arm
 
 def reference_prefix(n: int, m: int) -> np.ndarray:
@@ -257,8 +267,7 @@ def run_reference(args):
             "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.n / value * 1000.0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "10M x 100 f32 subspace mixture, k=100, leaf<=1024 (sampled prefix on CPU)",
-                       "reps": args.reps, "refine_passes": args.refine, "lloyd_iters": LLOYD_ITERS},
+            "config": workload_config(args.n, args.reps, args.refine, MAX_LEAF, False, args.gpus),
             "cpu_baseline": {"value": value, "unit": "points/s", "cores": res["cores"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -632,12 +641,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{n:,} x {DIM} f32, 1024-cluster Zipf(1.1) 24-d subspace mixture (seed {SEED}), "
-                                   f"k={K}, leaf<={max_leaf - 1}, {args.reps} repetitions, {LLOYD_ITERS} Lloyd "
-                                   f"iterations, {args.refine} neighbour-of-neighbour passes"
-                                   + (", BF16 bucket estimates + FP32 re-rank" if args.bf16 else ", FP32"),
-                       "n": n, "k": K, "reps": args.reps, "precision": "bf16_rerank" if args.bf16 else "fp32", "parallelism": f"replicas x{world}",
-                       "l2": "input 4 GB > 126 MB L2; no flush between steps"},
+            "config": workload_config(n, args.reps, args.refine, max_leaf, args.bf16, world),
             "recall": rec, "recall_queries": len(q), "meets_recall_target": rec >= 0.94,
             "clocks": clock, "gpu_launches": launches, "stream_ms_total": stream_ms, "wall_s": wall,
             "roofline": roofline, "e2e": e2e,
