@@ -27,6 +27,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "admission.hpp"
 #include "knng.h"
 
 namespace {
@@ -105,8 +106,8 @@ void worker_loop(knng_server* s) {
         // reservation fits and a running slot is free.
         s->cv_work.wait(lk, [s] {
             if (s->stopping) return true;
-            if (s->queue.empty() || s->running >= s->max_running) return false;
-            return s->in_use + s->queue.front()->need <= s->budget;
+            if (s->queue.empty()) return false;
+            return knng::admits(s->in_use, s->queue.front()->need, s->budget, s->running, s->max_running);
         });
         if (s->stopping) return;
         Job* j = s->queue.front();
