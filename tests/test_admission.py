@@ -50,8 +50,8 @@ def test_admission_rule_and_arrival_order(tmp_path):
     assert r.returncode == 0, "truth table"
     spans = [tuple(map(int, line.split())) for line in r.stdout.split("\n") if line.strip()]
     # job 0 (6) and job 1 (3) start at once; job 2 (8) waits until both have
-    # ended (t = 3), job 3 (1) then fits beside it; job 4 (4) waits for room
-    # (t = 5) although the budget would have fitted it earlier behind no one.
+    # ended (t = 3), job 3 (1) then fits beside it; job 4 (4) waits until job 2
+    # has ended and there is room (t = 5).
     assert spans == [(0, 3), (0, 1), (3, 5), (3, 4), (5, 7)]
     starts = [s for s, _ in spans]
     assert starts == sorted(starts)  # arrival order
