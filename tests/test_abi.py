@@ -78,6 +78,7 @@ int main() {
     std::vector<std::vector<uint32_t>> result;
     try {
         knng_b200::constructResult(pts, 4, result);
+        knng_b200::constructResultTimed(pts, 4, result, 50, 50);
     } catch (const std::runtime_error& e) {
         std::printf("%s\n", e.what());
         return 3;
