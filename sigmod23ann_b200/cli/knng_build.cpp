@@ -1,6 +1,12 @@
 // knng_build -- the reference's command line (src/main.cpp:39-71) on the GPU:
 //
 //   knng_build [input.bin] [output.bin] [reps] [refine passes] [max_leaf]
+//   knng_build input.bin output.bin --timed build_ms refine_ms
+//
+// The second form is the reference's wall-clock schedule
+// (SolutionKmeans::constructResult, src/SolutionKmeans.hpp:579-604):
+// repetitions while build_ms has not passed, then passes while
+// build_ms + refine_ms has not (the reference: 1,210,000 and 500,000 ms).
 //
 // input.bin: uint32 N, then N rows of 100 float32 (the contest format read by
 // ReadBinArray, src/io.h:66-95).  output.bin: N rows of 100 uint32 neighbour
@@ -21,9 +27,21 @@ int main(int argc, char** argv) {
     const std::string out = argc > 2 ? argv[2] : "output.bin";
     knng_params p;
     knng_default_params(&p);
-    if (argc > 3) p.reps = static_cast<uint32_t>(std::atoi(argv[3]));
-    if (argc > 4) p.refine = static_cast<uint32_t>(std::atoi(argv[4]));
-    if (argc > 5) {
+    const bool timed = argc > 3 && std::string(argv[3]) == "--timed";
+    uint64_t build_ms = 0, refine_ms = 0;
+    if (timed) {
+        if (argc < 6) {
+            std::fprintf(stderr, "usage: knng_build input.bin output.bin --timed build_ms refine_ms\n");
+            return 2;
+        }
+        build_ms = std::strtoull(argv[4], nullptr, 10);
+        refine_ms = std::strtoull(argv[5], nullptr, 10);
+        p.reps = 0;  // no cap: the clock decides
+    } else if (argc > 3) {
+        p.reps = static_cast<uint32_t>(std::atoi(argv[3]));
+    }
+    if (!timed && argc > 4) p.refine = static_cast<uint32_t>(std::atoi(argv[4]));
+    if (!timed && argc > 5) {
         p.max_leaf = static_cast<uint32_t>(std::atoi(argv[5]));
         p.max_leaf_odd = 0;
     }
@@ -49,7 +67,8 @@ int main(int argc, char** argv) {
     }
     std::vector<uint32_t> ids(static_cast<size_t>(n) * p.k);
     knng_stats st;
-    s = knng_build(ctx, pts.data(), n, 100, 400, &p, ids.data(), nullptr, &st);
+    s = timed ? knng_build_timed(ctx, pts.data(), n, 100, 400, &p, build_ms, refine_ms, ids.data(), nullptr, &st)
+              : knng_build(ctx, pts.data(), n, 100, 400, &p, ids.data(), nullptr, &st);
     if (s != KNNG_OK) {
         std::fprintf(stderr, "knng_build: %s: %s\n", knng_status_string(s), knng_last_error(ctx));
         knng_destroy(ctx);
@@ -59,7 +78,9 @@ int main(int argc, char** argv) {
     std::ofstream o(out, std::ios::binary);
     o.write(reinterpret_cast<const char*>(ids.data()), static_cast<std::streamsize>(ids.size() * sizeof(uint32_t)));
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    std::printf("points %u  reps %u  refine passes %u  device ms %.1f  total ms %.1f  -> %s\n", n, p.reps, p.refine,
-                st.ms_total + st.ms_finalize, ms, out.c_str());
+    std::printf("points %u  reps %llu  refine passes %llu  device ms %.1f  total ms %.1f  -> %s\n", n,
+                static_cast<unsigned long long>(st.reps_done),
+                static_cast<unsigned long long>(st.refine_join_launches), st.ms_total + st.ms_finalize, ms,
+                out.c_str());
     return 0;
 }

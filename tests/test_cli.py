@@ -41,6 +41,12 @@ def test_build_cli_without_device(knng_lib, tmp_path):
     r = subprocess.run([os.path.join(CLI, "knng_build"), str(tmp_path / "in.bin"), str(tmp_path / "out.bin")],
                        capture_output=True, text=True)
     assert r.returncode == 3 and "no sm_100" in r.stderr
+    r = subprocess.run([os.path.join(CLI, "knng_build"), str(tmp_path / "in.bin"), str(tmp_path / "out.bin"),
+                        "--timed", "100", "100"], capture_output=True, text=True)
+    assert r.returncode == 3 and "no sm_100" in r.stderr
+    r = subprocess.run([os.path.join(CLI, "knng_build"), str(tmp_path / "in.bin"), str(tmp_path / "out.bin"),
+                        "--timed", "100"], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
 
 
 @pytest.mark.gpu
