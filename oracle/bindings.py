@@ -21,7 +21,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libknng_oracle.so")
 REF_SERIAL_SO = os.path.join(HERE, "_ref", "libref_serial.so")
 REF_THREADS_SO = os.path.join(HERE, "_ref", "libref_threads.so")
-REFERENCE_SRC = "/root/reference/src"
+# The reference's source tree: KNNG_REFERENCE_SRC, else beside this
+# repository (../reference/src from its root).
+REFERENCE_SRC = os.environ.get("KNNG_REFERENCE_SRC",
+                               os.path.normpath(os.path.join(HERE, "..", "..", "reference", "src")))
+# The reference's own test fixture (u32 N, then N x 100 float32), beside its sources.
+REFERENCE_FIXTURE = os.path.join(os.path.dirname(REFERENCE_SRC), "dummy-data.bin")
 
 
 def build(with_reference: bool | None = None) -> None:
@@ -75,6 +80,8 @@ def _olib():
         lib.ko_leaf_count.argtypes = [c_void_p]
         lib.ko_leaf_count.restype = c_uint32
         lib.ko_leaves.argtypes = [c_void_p, c_void_p, c_void_p]
+        lib.ko_lloyd.argtypes = [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]
+        lib.ko_lloyd.restype = ctypes.c_int
         lib.ko_distance.argtypes = [c_void_p, c_void_p, c_uint32]
         lib.ko_distance.restype = c_float
         lib.ko_dot.argtypes = [c_void_p, c_void_p, c_uint32]
@@ -155,6 +162,17 @@ class Oracle:
 
     def refine(self) -> int:
         return int(self._lib.ko_refine(self._h))
+
+    def lloyd(self, ids: np.ndarray, c1: np.ndarray, c2: np.ndarray, iters: int):
+        """Lloyd steps over the point ids in the given order from centres c1, c2;
+        returns (coefs, offset, ok)."""
+        a = np.ascontiguousarray(ids, np.uint32)
+        x = np.ascontiguousarray(c1, np.float32)
+        y = np.ascontiguousarray(c2, np.float32)
+        coefs = np.zeros(self.d, np.float32)
+        off = np.zeros(1, np.float32)
+        ok = self._lib.ko_lloyd(self._h, _ptr(a), len(a), _ptr(x), _ptr(y), iters, _ptr(coefs), _ptr(off))
+        return coefs, off[0], bool(ok)
 
     def process_leaves(self, starts: np.ndarray, ends: np.ndarray) -> None:
         s = np.ascontiguousarray(starts, np.uint32)

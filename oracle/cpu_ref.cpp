@@ -579,6 +579,22 @@ void ko_leaves(void* h, uint32_t* starts, uint32_t* ends) {
     }
 }
 
+// `iters` Lloyd steps over the point ids ids[0..count) in that order from the
+// centres c1 / c2 (src/SolutionKmeans.hpp:161-186), then the final hyperplane;
+// returns 0 when a step left one side empty.
+int ko_lloyd(void* h, const uint32_t* ids, uint64_t count, const float* c1_in, const float* c2_in, uint32_t iters,
+             float* out_coefs, float* out_offset) {
+    const Oracle& o = *static_cast<Oracle*>(h);
+    std::vector<uint32_t> list(ids, ids + count);
+    std::vector<float> c1(c1_in, c1_in + o.d), c2(c2_in, c2_in + o.d);
+    for (uint32_t it = 0; it < iters; ++it)
+        if (!lloyd_step(o, list, c1, c2)) return 0;
+    std::vector<float> coefs;
+    hyperplane(c1, c2, o.d, coefs, *out_offset);
+    std::copy(coefs.begin(), coefs.end(), out_coefs);
+    return 1;
+}
+
 float ko_distance(const float* a, const float* b, uint32_t d) { return canonical_distance(a, b, d); }
 
 float ko_dot(const float* a, const float* b, uint32_t d) { return canonical_dot(a, b, d); }

@@ -335,15 +335,17 @@ std::vector<uint32_t> split_level(Context& c, const std::vector<Node>& active, u
         launch_draw_positions(c, cnt, d_s, d_e, d_b, d_a, d_doff, d_sb, d_loff, seed, rep, seeds, lloyd);
         uint32_t* first = static_cast<uint32_t*>(scratch(c, "lvl_first", cnt * sizeof(uint32_t)));
         uint32_t* second = static_cast<uint32_t*>(scratch(c, "lvl_second", cnt * sizeof(uint32_t)));
-        int32_t* ok = static_cast<int32_t*>(scratch(c, "lvl_ok", cnt * sizeof(int32_t)));
+        // ok[t]: node t seeded and converged; ok[cnt]: a Lloyd wait gave up.
+        int32_t* ok = static_cast<int32_t*>(scratch(c, "lvl_ok", (cnt + 1) * sizeof(int32_t)));
         float* c1 = static_cast<float*>(scratch(c, "lvl_c1", static_cast<size_t>(cnt) * ld * sizeof(float)));
         float* c2 = static_cast<float*>(scratch(c, "lvl_c2", static_cast<size_t>(cnt) * ld * sizeof(float)));
         float* coefs = static_cast<float*>(scratch(c, "lvl_coefs", static_cast<size_t>(cnt) * ld * sizeof(float)));
         float* offs = static_cast<float*>(scratch(c, "lvl_offsets", cnt * sizeof(float)));
         launch_farthest_pair(c, cnt, d_sb, seeds, max_seed, first, second, ok, c1, c2);
         launch_lloyd(c, cnt, hs.data(), he.data(), lloyd_off.data(), lloyd, c1, c2, lloyd_iters, coefs, offs, ok);
-        std::vector<int32_t> hok(cnt);
-        download(c, hok.data(), ok, cnt);
+        std::vector<int32_t> hok(cnt + 1);
+        download(c, hok.data(), ok, cnt + 1);
+        if (hok[cnt]) fail(KNNG_ERR_CUDA, "Lloyd sums: a bulk-copy wait gave up");
         // Partition the nodes that seeded and converged.
         std::vector<uint32_t> sel;
         for (uint32_t t = 0; t < cnt; ++t) {
@@ -734,8 +736,8 @@ knng_status knng_lloyd(knng_context* ctx, uint32_t count, const uint32_t* starts
         float* d1 = knng::upload(c, "ll_c1", h1.data(), h1.size());
         float* d2 = knng::upload(c, "ll_c2", h2.data(), h2.size());
         uint32_t* d_pos = knng::upload(c, "ll_pos", lloyd_positions, total);
-        std::vector<int32_t> ones(count, 1);
-        int32_t* d_ok = knng::upload(c, "ll_ok", ones.data(), count);
+        std::vector<int32_t> ones(count + 1, 1);
+        int32_t* d_ok = knng::upload(c, "ll_ok", ones.data(), count + 1);
         float* d_coefs = static_cast<float*>(knng::scratch(c, "ll_coefs", static_cast<size_t>(count) * ld * sizeof(float)));
         float* d_offs = static_cast<float*>(knng::scratch(c, "ll_offs", count * sizeof(float)));
         knng::launch_lloyd(c, count, starts, ends, lloyd_offsets, d_pos, d1, d2, iters, d_coefs, d_offs, d_ok);
@@ -744,7 +746,10 @@ knng_status knng_lloyd(knng_context* ctx, uint32_t count, const uint32_t* starts
         for (uint32_t i = 0; i < count; ++i)
             std::memcpy(out_coefs + static_cast<size_t>(i) * c.d, &hc[static_cast<size_t>(i) * ld], c.d * sizeof(float));
         knng::download(c, out_offsets, d_offs, count);
-        knng::download(c, out_ok, d_ok, count);
+        std::vector<int32_t> hok(count + 1);
+        knng::download(c, hok.data(), d_ok, count + 1);
+        if (hok[count]) knng::fail(KNNG_ERR_CUDA, "Lloyd sums: a bulk-copy wait gave up");
+        std::memcpy(out_ok, hok.data(), count * sizeof(int32_t));
     });
 }
 

@@ -6,10 +6,12 @@
 //                      (getSampleFromPercent :55-66, kmeansStartVecs :103-111)
 //   k_farthest_pair    farthest pair among the seed positions (:68-101, :113-127)
 //   k_plane            between / coefs / offset from two centres (:162-164)
-//   k_lloyd_accum      side test + per-cluster double sums over a tile
-//                      (:170-175, :227-238)
-//   k_lloyd_reduce     per-node sum of tile partials, new centres (:182-185, :239-259)
-//   k_side             final side test of every point of a node (:195-197, :273-278)
+//   k_side             side test of a node's Lloyd set (:170-175, :227-238) or
+//                      of its whole range (:195-197, :273-278), eight lanes
+//                      per point in the reference's FMA-chain order
+//   k_lloyd_seq        per-side double sums in the Lloyd set's order and the
+//                      new centres (:170-186, :227-259), one CTA per node fed
+//                      by bulk copies
 //   k_scan_items       exclusive scan of per-tile side-true counts
 //   k_scatter          stable partition, side-true first (std::stable_partition
 //                      at :195, the group memcpy at :301-304)
@@ -27,6 +29,7 @@
 #include "common.cuh"
 #include "context.hpp"
 #include "dispatch.hpp"
+#include "tc.cuh"
 
 namespace knng {
 namespace {
@@ -34,15 +37,17 @@ namespace {
 constexpr int kSideThreads = 256;
 constexpr int kSidePer = 8;  // positions per thread in the side / scatter kernels
 constexpr int kChunk = kSideThreads * kSidePer;
-constexpr int kLloydThreads = 256;
-constexpr int kLloydTile = 64;
-constexpr int kLloydItem = 256;  // positions per Lloyd work item
 constexpr int kPairThreads = 256;
+constexpr uint32_t kListItem = 0x80000000u;  // Item::node flag: entries come from a position list
 
+// A chunk of one node's entries: positions begin .. begin+count (range item)
+// or list[begin .. begin+count) (list item, kListItem set in `node`).  The
+// side kernel writes entry r's flag at fbase + r.
 struct Item {
     uint32_t node;
     uint32_t count;
-    uint64_t begin;  // first position (range items) or first list entry (list items)
+    uint64_t begin;
+    uint64_t fbase;
 };
 
 __global__ void k_iota(uint32_t* __restrict__ idx, uint32_t n) {
@@ -190,122 +195,243 @@ __global__ void k_plane(const float* __restrict__ c1, const float* __restrict__ 
     if (lane == 0) offsets[node] = canonical_dot<D>(between, coefs + base);
 }
 
-// Per work item: side test of up to kLloydItem points against the node's
-// current hyperplane, then per-cluster double sums in point order.
-// partial layout per item: [n1, n2, s1[0..D), s2[0..D)].
+// ------------------------------------------------------------ side test
+//
+// Eight lanes test one point: lane l of the group runs FMA chain l of the
+// reference's dot (dims l, l+8, ... below the largest multiple of 8), the
+// group's lanes are then summed left to right into 0.0f and the tail dims
+// added as separately rounded products -- the order of `dot`
+// (src/LinearAlgebra.hpp:179-200).  A warp tests four points at a time; each
+// of its scalar loads reads a whole 32-byte sector of each point's row.
+
+// The hyperplane values FMA chain l needs (chain steps, then the tail).
 template <int D>
-__global__ void __launch_bounds__(kLloydThreads) k_lloyd_accum(const Item* __restrict__ items,
-                                                               const uint32_t* __restrict__ list,
-                                                               const uint32_t* __restrict__ idx,
-                                                               const float* __restrict__ pts, int ld,
-                                                               const float* __restrict__ coefs,
-                                                               const float* __restrict__ offsets,
-                                                               double* __restrict__ partial) {
-    constexpr int Q = (D + 3) / 4;
-    __shared__ float4 rows[kLloydTile][Q];
-    __shared__ float4 plane[Q];
-    __shared__ int side[kLloydTile];
-    const Item it = items[blockIdx.x];
-    const bool from_list = (it.node & 0x80000000u) != 0;
-    const uint32_t node = it.node & 0x7FFFFFFFu;
-    for (int q = threadIdx.x; q < Q; q += blockDim.x)
-        plane[q] = reinterpret_cast<const float4*>(coefs + static_cast<size_t>(node) * ld)[q];
-    const float off = offsets[node];
-    const int t = threadIdx.x;
-    const int cluster = t / D;  // 0: side-true sums, 1: side-false sums, >= 2 idle
-    const int dim = t % D;
-    double acc = 0.0;
-    uint32_t cnt = 0;
-    for (uint32_t base = 0; base < it.count; base += kLloydTile) {
-        const uint32_t rows_here = min(static_cast<uint32_t>(kLloydTile), it.count - base);
-        __syncthreads();
-        for (uint32_t f = threadIdx.x; f < rows_here * Q; f += blockDim.x) {
-            const uint32_t r = f / Q, q = f % Q;
-            const uint64_t e = it.begin + base + r;
-            const uint32_t pos = from_list ? list[e] : static_cast<uint32_t>(e);
-            rows[r][q] = reinterpret_cast<const float4*>(pts + static_cast<size_t>(idx[pos]) * ld)[q];
-        }
-        __syncthreads();
-        if (t < static_cast<int>(rows_here)) side[t] = canonical_dot4<D>(plane, rows[t]) >= off ? 1 : 0;
-        __syncthreads();
-        if (cluster < 2) {
-            const int want = cluster == 0 ? 1 : 0;
-            const float* rf = reinterpret_cast<const float*>(rows);
-            for (uint32_t r = 0; r < rows_here; ++r) {
-                if (side[r] == want) {
-                    acc = __dadd_rn(acc, static_cast<double>(rf[r * Q * 4 + dim]));
-                    ++cnt;
-                }
-            }
-        }
-    }
-    double* out = partial + static_cast<size_t>(blockIdx.x) * (2 * D + 2);
-    if (cluster < 2) {
-        out[2 + cluster * D + dim] = acc;
-        if (dim == 0) out[cluster] = static_cast<double>(cnt);
-    }
+struct ChainPlane {
+    static constexpr int M = D / 8 * 8;
+    float c[M / 8 > 0 ? M / 8 : 1];
+    float4 tail;
+};
+
+template <int D>
+__device__ __forceinline__ void load_chain_plane(ChainPlane<D>& p, const float* __restrict__ coefs_row, int l) {
+    constexpr int M = ChainPlane<D>::M;
+#pragma unroll
+    for (int i = 0; i < M / 8; ++i) p.c[i] = coefs_row[8 * i + l];
+    p.tail = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (D > M) p.tail = *reinterpret_cast<const float4*>(coefs_row + M);
 }
 
-// Per node: items [item_begin, item_end) summed in order; centres updated.
+// dot(coefs, row) in the reference's order, by the eight lanes of the group
+// whose first lane is `g0`; every lane of the group returns the result.  All
+// 32 lanes must call it together.
 template <int D>
-__global__ void k_lloyd_reduce(const uint32_t* __restrict__ item_begin, const uint32_t* __restrict__ item_end,
-                               const double* __restrict__ partial, int ld, float* __restrict__ c1,
-                               float* __restrict__ c2, int32_t* __restrict__ ok) {
-    const uint32_t node = blockIdx.x;
-    const uint32_t ib = item_begin[node], ie = item_end[node];
-    __shared__ double counts[2];
-    if (threadIdx.x < 2) {
-        double c = 0.0;
-        for (uint32_t i = ib; i < ie; ++i) c = __dadd_rn(c, partial[static_cast<size_t>(i) * (2 * D + 2) + threadIdx.x]);
-        counts[threadIdx.x] = c;
+__device__ __forceinline__ float group_dot(const ChainPlane<D>& p, const float* __restrict__ row, int l, int g0) {
+    constexpr int M = ChainPlane<D>::M;
+    static_assert(D - M == 0 || D - M == 4, "tail of 0 or 4 dims");
+    float chain = 0.0f;
+#pragma unroll
+    for (int i = 0; i < M / 8; ++i) chain = __fmaf_rn(__ldg(row + 8 * i + l), p.c[i], chain);
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc = __fadd_rn(acc, __shfl_sync(kFull, chain, g0 + j));
+    if constexpr (D > M) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(row + M));
+        acc = __fadd_rn(acc, __fmul_rn(p.tail.x, x.x));
+        acc = __fadd_rn(acc, __fmul_rn(p.tail.y, x.y));
+        acc = __fadd_rn(acc, __fmul_rn(p.tail.z, x.z));
+        acc = __fadd_rn(acc, __fmul_rn(p.tail.w, x.w));
     }
-    __syncthreads();
-    const double n1 = counts[0], n2 = counts[1];
-    if (threadIdx.x == 0 && (n1 == 0.0 || n2 == 0.0)) ok[node] = 0;
-    for (int t = threadIdx.x; t < 2 * D; t += blockDim.x) {
-        const int cluster = t / D, dim = t % D;
-        double s = 0.0;
-        for (uint32_t i = ib; i < ie; ++i) s = __dadd_rn(s, partial[static_cast<size_t>(i) * (2 * D + 2) + 2 + t]);
-        const double nn = cluster == 0 ? n1 : n2;
-        if (nn > 0.0) {
-            const float v = __double2float_rn(__ddiv_rn(s, nn));
-            (cluster == 0 ? c1 : c2)[static_cast<size_t>(node) * ld + dim] = v;
-        }
-    }
+    return acc;
 }
 
-// Side flags for the positions of one chunk of one node; per-chunk true count.
+// Side flags of one item (up to kChunk entries of one node): entry r reads
+// position begin + r, or list[begin + r] for a list item; its flag goes to
+// flags[fbase + r] and, when `ids_out` is given, its point id to
+// ids_out[fbase + r].  item_true[item] = the item's side-true count.
 template <int D>
-__global__ void __launch_bounds__(kSideThreads) k_side(const Item* __restrict__ items, const uint32_t* __restrict__ idx,
-                                                       const float* __restrict__ pts, int ld,
-                                                       const float* __restrict__ coefs,
-                                                       const float* __restrict__ offsets,
-                                                       uint8_t* __restrict__ flags, uint32_t* __restrict__ item_true) {
-    constexpr int Q = (D + 3) / 4;
-    __shared__ float4 plane[Q];
+__global__ void __launch_bounds__(kSideThreads) k_side(const Item* __restrict__ items, const uint32_t* __restrict__ list,
+                                                       const uint32_t* __restrict__ idx, const float* __restrict__ pts,
+                                                       int ld, const float* __restrict__ coefs,
+                                                       const float* __restrict__ offsets, uint8_t* __restrict__ flags,
+                                                       uint32_t* __restrict__ ids_out,
+                                                       uint32_t* __restrict__ item_true) {
     __shared__ uint32_t warp_sum[kSideThreads / kWarp];
     const Item it = items[blockIdx.x];
-    for (int q = threadIdx.x; q < Q; q += blockDim.x)
-        plane[q] = reinterpret_cast<const float4*>(coefs + static_cast<size_t>(it.node) * ld)[q];
-    const float off = offsets[it.node];
-    __syncthreads();
+    const bool from_list = (it.node & kListItem) != 0;
+    const uint32_t node = it.node & ~kListItem;
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    const int l = lane & 7, grp = lane >> 3, g0 = lane & ~7;
+    ChainPlane<D> plane;
+    load_chain_plane<D>(plane, coefs + static_cast<size_t>(node) * ld, l);
+    const float off = offsets[node];
     uint32_t cnt = 0;
-    for (uint32_t r = threadIdx.x; r < it.count; r += blockDim.x) {
-        const uint64_t pos = it.begin + r;
-        const float4* row = reinterpret_cast<const float4*>(pts + static_cast<size_t>(idx[pos]) * ld);
-        const uint8_t f = canonical_dot4<D>(plane, row) >= off ? 1 : 0;
-        flags[pos] = f;
-        cnt += f;
-    }
+    // Each warp takes 32 consecutive entries at a time.
+    for (uint32_t r0 = warp * kWarp; r0 < it.count; r0 += kSideThreads) {
+        const uint32_t r = r0 + lane;
+        uint32_t id = 0;
+        if (r < it.count) {
+            const uint64_t e = it.begin + r;
+            id = idx[from_list ? list[e] : static_cast<uint32_t>(e)];
+        }
+        uint32_t mask = 0;  // bit j: entry r0 + j is side-true
+#pragma unroll 1
+        for (int b = 0; b < 8; ++b) {
+            const int j = 4 * b + grp;
+            const uint32_t pid = __shfl_sync(kFull, id, j);
+            const float v = group_dot<D>(plane, pts + static_cast<size_t>(pid) * ld, l, g0);
+            const bool f = r0 + j < it.count && v >= off;
+            const unsigned bal = __ballot_sync(kFull, f && l == 0);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
-    if (threadIdx.x % kWarp == 0) warp_sum[threadIdx.x / kWarp] = cnt;
+            for (int q = 0; q < 4; ++q) mask |= ((bal >> (8 * q)) & 1u) << (4 * b + q);
+        }
+        if (r < it.count) {
+            const uint8_t f = (mask >> lane) & 1u;
+            flags[it.fbase + r] = f;
+            if (ids_out) ids_out[it.fbase + r] = id;
+        }
+        cnt += __popc(mask);  // warp-uniform
+    }
+    if (lane == 0) warp_sum[warp] = cnt;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t s = 0;
         for (int w = 0; w < kSideThreads / kWarp; ++w) s += warp_sum[w];
         item_true[blockIdx.x] = s;
     }
+}
+
+// ------------------------------------------------------------- Lloyd sums
+//
+// The new centres are the per-side means of the node's Lloyd set, summed in
+// double one point at a time in the set's order (src/SolutionKmeans.hpp:
+// 170-175, :227-238 -- under a serial scheduler the large-node combinable
+// holds one partial, so that order is the sample's).  Rounding makes that
+// sum order-dependent, so it is not split: one CTA per node walks the set in
+// order.  A producer warp streams the rows into shared memory with bulk
+// copies (one per row, into a ring of kSeqStages tiles on mbarriers); warp 0
+// sums the side-true rows and warp 1 the side-false rows, each lane owning
+// dims lane, lane+32, ... so a node's 2*D sums advance together.
+constexpr int kSeqRows = 64;
+constexpr int kSeqStages = 4;
+constexpr int kSeqThreads = 3 * kWarp;
+
+struct SeqNode {
+    uint64_t fbase;  // first entry of the node in the flag / id arrays (16-byte aligned)
+    uint32_t len;    // entries
+    uint32_t pad;
+};
+
+__host__ __device__ constexpr size_t seq_smem_bytes(int D) {
+    return static_cast<size_t>(kSeqStages) * kSeqRows * D * sizeof(float) + kSeqStages * kSeqRows;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kSeqThreads) k_lloyd_seq(const SeqNode* __restrict__ nodes,
+                                                           const uint8_t* __restrict__ flags,
+                                                           const uint32_t* __restrict__ ids,
+                                                           const float* __restrict__ pts, int ld, float* __restrict__ c1,
+                                                           float* __restrict__ c2, int32_t* __restrict__ ok,
+                                                           int32_t* __restrict__ error_flag) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float* tiles = reinterpret_cast<float*>(smem);                                   // [stage][row][D]
+    uint8_t* tflags = smem + static_cast<size_t>(kSeqStages) * kSeqRows * D * 4;  // [stage][row]
+    __shared__ uint64_t full[kSeqStages], empty[kSeqStages];
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    const uint32_t node = blockIdx.x;
+    const SeqNode nd = nodes[node];
+    const uint32_t ntiles = (nd.len + kSeqRows - 1) / kSeqRows;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kSeqStages; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 2);
+        }
+        tc::fence_barrier_init();
+    }
+    __syncthreads();
+    constexpr uint32_t kRowBytes = D * sizeof(float);
+    if (warp == 2) {
+        // Producer: ids of the next tile are loaded while this one is issued.
+        uint32_t next[kSeqRows / kWarp];
+        auto load_ids = [&](uint32_t t) {
+#pragma unroll
+            for (int u = 0; u < kSeqRows / kWarp; ++u) {
+                const uint32_t e = t * kSeqRows + lane + u * kWarp;
+                next[u] = (t < ntiles && e < nd.len) ? ids[nd.fbase + e] : 0u;
+            }
+        };
+        load_ids(0);
+        uint32_t issued = 0;
+        for (uint32_t t = 0; t < ntiles; ++t) {
+            uint32_t cur[kSeqRows / kWarp];
+#pragma unroll
+            for (int u = 0; u < kSeqRows / kWarp; ++u) cur[u] = next[u];
+            load_ids(t + 1);
+            const uint32_t s = t % kSeqStages;
+            if (t >= kSeqStages && !tc::mbar_wait_limited(&empty[s], ((t / kSeqStages) - 1) & 1u)) {
+                if (lane == 0) atomicExch(error_flag, 1);
+                break;
+            }
+            const uint32_t rows = min(static_cast<uint32_t>(kSeqRows), nd.len - t * kSeqRows);
+            const uint32_t fbytes = (rows + 15u) & ~15u;
+            if (lane == 0) tc::mbar_arrive_expect_tx(&full[s], rows * kRowBytes + fbytes);
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < kSeqRows / kWarp; ++u) {
+                const uint32_t r = lane + u * kWarp;
+                if (r < rows)
+                    tc::bulk_g2s(tiles + (static_cast<size_t>(s) * kSeqRows + r) * D,
+                                 pts + static_cast<size_t>(cur[u]) * ld, kRowBytes, &full[s]);
+            }
+            if (lane == 0) tc::bulk_g2s(tflags + s * kSeqRows, flags + nd.fbase + t * kSeqRows, fbytes, &full[s]);
+            issued = t + 1;
+        }
+        // No copy may be in flight when the CTA exits.
+        const uint32_t first = issued > kSeqStages ? issued - kSeqStages : 0u;
+        for (uint32_t t = first; t < issued; ++t)
+            if (!tc::mbar_wait(&full[t % kSeqStages], (t / kSeqStages) & 1u) && lane == 0) atomicExch(error_flag, 1);
+        return;
+    }
+    // Consumers: warp 0 sums the side-true rows, warp 1 the side-false rows.
+    const uint8_t want = warp == 0 ? 1 : 0;
+    constexpr int PER = (D + kWarp - 1) / kWarp;
+    double acc[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) acc[j] = 0.0;
+    uint32_t cnt = 0;
+    bool healthy = true;
+    for (uint32_t t = 0; t < ntiles; ++t) {
+        const uint32_t s = t % kSeqStages;
+        if (!tc::mbar_wait_limited(&full[s], (t / kSeqStages) & 1u)) {
+            if (lane == 0) atomicExch(error_flag, 1);
+            healthy = false;
+            break;
+        }
+        const uint32_t rows = min(static_cast<uint32_t>(kSeqRows), nd.len - t * kSeqRows);
+        const float* tile = tiles + static_cast<size_t>(s) * kSeqRows * D;
+        const uint8_t* tf = tflags + s * kSeqRows;
+#pragma unroll 4
+        for (uint32_t r = 0; r < rows; ++r) {
+            if (tf[r] == want) {
+#pragma unroll
+                for (int j = 0; j < PER; ++j)
+                    if (lane + j * kWarp < D)
+                        acc[j] = __dadd_rn(acc[j], static_cast<double>(tile[r * D + lane + j * kWarp]));
+                ++cnt;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[s]);
+    }
+    if (!healthy) return;
+    if (cnt == 0) {
+        if (lane == 0) ok[node] = 0;
+        return;
+    }
+    float* c = (warp == 0 ? c1 : c2) + static_cast<size_t>(node) * ld;
+    const double nn = static_cast<double>(cnt);
+#pragma unroll
+    for (int j = 0; j < PER; ++j)
+        if (lane + j * kWarp < D) c[lane + j * kWarp] = __double2float_rn(__ddiv_rn(acc[j], nn));
 }
 
 // Exclusive scan of n values into out[0..n] (out[n] = total); one CTA.
@@ -460,32 +586,41 @@ void launch_lloyd(Context& c, uint32_t count, const uint32_t* h_starts, const ui
                   const uint64_t* h_lloyd_offsets, const uint32_t* d_lloyd_positions, float* d_c1, float* d_c2,
                   uint32_t iters, float* d_coefs, float* d_offsets, int32_t* d_ok) {
     if (count == 0) return;
-    // Work items: each node's Lloyd set (its list, or its whole range when the
-    // list is empty) cut into kLloydItem-point items, in order.
+    // Each node's Lloyd set is its list (large nodes) or its whole range
+    // (small nodes).  Its entries get a 16-byte aligned block of the flag / id
+    // arrays (the bulk copies of the sums kernel read whole 16-byte pieces),
+    // and are cut into kChunk-entry items for the side kernel.
     std::vector<Item> items;
-    std::vector<uint32_t> ib(count), ie(count);
+    std::vector<SeqNode> nodes(count);
+    uint64_t fnext = 0;
     for (uint32_t i = 0; i < count; ++i) {
-        ib[i] = static_cast<uint32_t>(items.size());
         const uint64_t lb = h_lloyd_offsets[i], le = h_lloyd_offsets[i + 1];
-        if (le > lb) {
-            for (uint64_t o = lb; o < le; o += kLloydItem)
-                items.push_back({i | 0x80000000u, static_cast<uint32_t>(std::min<uint64_t>(kLloydItem, le - o)), o});
-        } else {
-            for (uint64_t o = h_starts[i]; o < h_ends[i]; o += kLloydItem)
-                items.push_back({i, static_cast<uint32_t>(std::min<uint64_t>(kLloydItem, h_ends[i] - o)), o});
-        }
-        ie[i] = static_cast<uint32_t>(items.size());
+        const bool from_list = le > lb;
+        const uint64_t b = from_list ? lb : h_starts[i];
+        const uint64_t len = from_list ? le - lb : static_cast<uint64_t>(h_ends[i] - h_starts[i]);
+        nodes[i] = {fnext, static_cast<uint32_t>(len), 0u};
+        for (uint64_t o = 0; o < len; o += kChunk)
+            items.push_back({i | (from_list ? kListItem : 0u), static_cast<uint32_t>(std::min<uint64_t>(kChunk, len - o)),
+                             b + o, fnext + o});
+        fnext += (len + 15) / 16 * 16;
     }
-    const Item* d_items = upload(c, "lloyd_items", items.data(), items.size());
-    const uint32_t* d_ib = upload(c, "lloyd_ib", ib.data(), count);
-    const uint32_t* d_ie = upload(c, "lloyd_ie", ie.data(), count);
+    const uint32_t ni = static_cast<uint32_t>(items.size());
+    const Item* d_items = upload(c, "lloyd_items", items.data(), ni);
+    const SeqNode* d_nodes = upload(c, "lloyd_nodes", nodes.data(), count);
+    uint8_t* flags = static_cast<uint8_t*>(scratch(c, "lloyd_flags", fnext + 64));
+    uint32_t* ids = static_cast<uint32_t*>(scratch(c, "lloyd_ids", (fnext + 64) * sizeof(uint32_t)));
+    uint32_t* item_true = static_cast<uint32_t*>(scratch(c, "lloyd_item_true", (ni + 1) * sizeof(uint32_t)));
+    int32_t* err = d_ok + count;
+    KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(int32_t), c.stream));
     KNNG_DISPATCH_D(c.d, {
-        double* partial = static_cast<double*>(scratch(c, "lloyd_partial", items.size() * (2 * D + 2) * sizeof(double)));
+        auto seq = k_lloyd_seq<D>;
+        allow_max_smem(c, seq);
         for (uint32_t iter = 0; iter < iters; ++iter) {
             launch_plane(c, count, d_c1, d_c2, d_coefs, d_offsets);
-            k_lloyd_accum<D><<<static_cast<uint32_t>(items.size()), kLloydThreads, 0, c.stream>>>(
-                d_items, d_lloyd_positions, c.indices, c.points, c.ld, d_coefs, d_offsets, partial);
-            k_lloyd_reduce<D><<<count, 256, 0, c.stream>>>(d_ib, d_ie, partial, c.ld, d_c1, d_c2, d_ok);
+            k_side<D><<<ni, kSideThreads, 0, c.stream>>>(d_items, d_lloyd_positions, c.indices, c.points, c.ld,
+                                                         d_coefs, d_offsets, flags, ids, item_true);
+            seq<<<count, kSeqThreads, seq_smem_bytes(D), c.stream>>>(d_nodes, flags, ids, c.points, c.ld, d_c1, d_c2,
+                                                                     d_ok, err);
             c.launches += 2;
             KNNG_CUDA(cudaGetLastError());
         }
@@ -501,7 +636,7 @@ void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, cons
     for (uint32_t i = 0; i < count; ++i) {
         ib[i] = static_cast<uint32_t>(items.size());
         for (uint64_t o = h_starts[i]; o < h_ends[i]; o += kChunk)
-            items.push_back({i, static_cast<uint32_t>(std::min<uint64_t>(kChunk, h_ends[i] - o)), o});
+            items.push_back({i, static_cast<uint32_t>(std::min<uint64_t>(kChunk, h_ends[i] - o)), o, o});
         ie[i] = static_cast<uint32_t>(items.size());
     }
     const uint32_t ni = static_cast<uint32_t>(items.size());
@@ -512,8 +647,8 @@ void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, cons
     uint32_t* item_true = static_cast<uint32_t*>(scratch(c, "item_true", (ni + 1) * sizeof(uint32_t)));
     uint32_t* prefix = static_cast<uint32_t*>(scratch(c, "item_prefix", (ni + 1) * sizeof(uint32_t)));
     KNNG_DISPATCH_D(c.d, {
-        k_side<D><<<ni, kSideThreads, 0, c.stream>>>(d_items, c.indices, c.points, c.ld, d_coefs, d_offsets, flags,
-                                                     item_true);
+        k_side<D><<<ni, kSideThreads, 0, c.stream>>>(d_items, nullptr, c.indices, c.points, c.ld, d_coefs, d_offsets,
+                                                     flags, nullptr, item_true);
     });
     k_scan_items<<<1, 1024, 0, c.stream>>>(item_true, ni, prefix);
     k_node_true<<<(count + 255) / 256, 256, 0, c.stream>>>(d_ib, d_ie, prefix, count, d_true);

@@ -43,6 +43,53 @@ __device__ __forceinline__ void fence_barrier_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Arrives once on the barrier and raises its expected transaction bytes.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Arrives once on the barrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bulk copy (the TMA engine's untiled form, this CTA's shared memory, no
+// multicast) of `bytes` from global memory; completes `bytes` transactions on
+// the barrier.  Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem_dst)),
+                 "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Poll limit of the waits for work in progress (mbar_wait_limited) in this
+// translation unit's kernels.  A diagnostic entry point may shorten it so a
+// test can make such a wait run out; waits that drain a kernel's own copies
+// before it exits always use kSpinLimit.
+static __device__ uint32_t g_wait_limit = kSpinLimit;
+
+__device__ __forceinline__ bool mbar_poll(uint32_t addr, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Waits for phase `parity` with this translation unit's poll limit.
+__device__ __forceinline__ bool mbar_wait_limited(uint64_t* bar, uint32_t parity) {
+    return mbar_poll(smem_u32(bar), parity, g_wait_limit);
+}
+
 // Polls phase `parity` of the barrier; returns false if the poll limit ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     const uint32_t addr = smem_u32(bar);

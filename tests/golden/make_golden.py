@@ -6,14 +6,18 @@ Boost / robin_set headers, serial scheduler):
 
     python tests/golden/make_golden.py
 
-The inputs are seeded synthetic point sets regenerated by the tests, so only
-the reference's outputs are stored: SHA-256 digests of whole arrays plus a
-few rows verbatim.
+The inputs are seeded synthetic point sets regenerated by the tests, plus
+the reference's own fixture dummy-data.bin (10,000 x 100, the input its
+main() reads by default), which this script stores beside golden.json as
+dummy-data.bin.xz so the GPU tests have it on a host without the reference
+tree.  Only the reference's outputs are stored for them: SHA-256 digests of
+whole arrays plus a few rows verbatim.
 """
 from __future__ import annotations
 
 import hashlib
 import json
+import lzma
 import os
 import sys
 
@@ -25,10 +29,16 @@ sys.path.insert(0, ROOT)
 from oracle import bindings  # noqa: E402
 from sigmod23ann_b200 import workloads  # noqa: E402
 
-OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "golden.json")
+FIXTURE = "dummy-data.bin.xz"
 
-# (name, generator kwargs, [(lloyd iterations, maxGroupSize) per repetition], top-up)
+# (name, generator kwargs or {"file": fixture}, [(lloyd iterations, maxGroupSize) per repetition], top-up)
 CASES = [
+    # The reference's schedule on its own fixture: one Lloyd iteration
+    # (src/SolutionKmeans.hpp:591), buckets alternating below 200 / 400
+    # (:582-587), then the top-up (:604).
+    ("dummy_data", {"file": FIXTURE}, [(1, 200), (1, 400), (1, 200), (1, 400)], True),
     ("mix6k", dict(n=6000, d=100, clusters=16, sigma=0.15, seed=7), [(1, 200), (2, 400)], True),
     ("mix3500_leaf64", dict(n=3500, d=100, clusters=8, sigma=0.2, seed=11), [(2, 64)], True),
     ("mix250_one_bucket", dict(n=250, d=100, clusters=4, sigma=0.3, seed=5), [(1, 400)], False),
@@ -46,11 +56,24 @@ def sets_digest(s: dict) -> str:
     return h.hexdigest()
 
 
+def case_points(gen: dict) -> np.ndarray:
+    if "file" in gen:
+        with lzma.open(os.path.join(HERE, gen["file"])) as f:
+            raw = f.read()
+        n = int(np.frombuffer(raw[:4], np.uint32)[0])
+        return np.frombuffer(raw[4:4 + n * 400], np.float32).reshape(n, 100).copy()
+    return workloads.gaussian_mixture(**gen)
+
+
 def main() -> int:
     bindings.build(with_reference=True)
+    with open(bindings.REFERENCE_FIXTURE, "rb") as f:
+        raw = f.read()
+    with lzma.open(os.path.join(HERE, FIXTURE), "wb", preset=9) as f:
+        f.write(raw)
     golden = {"cases": {}, "arith": {}, "knnset": {}}
     for name, gen, reps, topup in CASES:
-        pts = workloads.gaussian_mixture(**gen)
+        pts = case_points(gen)
         ref = bindings.ReferenceShim(pts)
         ref.reseed(12345)
         entry = {"generator": gen, "reps": reps, "topup": topup, "indices": [], "sets": []}

@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import assert_sets_equal, digest, feed_trace, sets_digest
+from helpers import assert_sets_equal, case_points, digest, feed_trace, sets_digest
 from sigmod23ann_b200 import KnngContext, KnngError, default_params, workloads
 
 pytestmark = pytest.mark.gpu
@@ -44,7 +44,7 @@ def oracle_rep_and_feed(oracle_lib, ctx, pts, reps, k=100, check_each=True):
 def test_golden_cases_through_gpu(oracle_lib, ctx, golden):
     """Reference outputs (fixtures) reproduced by the GPU fed the hyperplanes."""
     for name, case in golden["cases"].items():
-        pts = workloads.gaussian_mixture(**case["generator"])
+        pts = case_points(case["generator"])
         o = oracle_lib.Oracle(pts, k=100, rng_mode=0, seed=12345)
         ctx.load_points(pts)
         ctx.reset_sets(100)
@@ -135,6 +135,34 @@ def test_farthest_pair_and_lloyd_parity(oracle_lib, ctx):
     np.testing.assert_array_equal(ctx.indices(), o.indices())
 
 
+def test_lloyd_sums_round_in_point_order(oracle_lib, ctx):
+    """Centroid sums whose partial sums round (values from 2^-45 to 2^8): the
+    device adds one point at a time in the Lloyd set's order, as the
+    reference does, so its hyperplanes equal the oracle's bit for bit; 256-point
+    partial sums would move dims 0 and 2 by one float ulp.  Covers a small
+    node (the whole range), a large node's position list, and a shuffled list
+    with repeats (samples are drawn with replacement)."""
+    from helpers import rounding_points
+
+    rng = np.random.default_rng(5)
+    shuffled = rng.integers(0, 1024, 3000).astype(np.uint32)
+    cases = [(1024, np.zeros(0, np.uint32)), (4096, np.arange(1024, dtype=np.uint32)), (4096, shuffled)]
+    for n, plist in cases:
+        pts = rounding_points(n)
+        ctx.load_points(pts)
+        ctx.reset_sets(10)
+        ctx.begin_rep()
+        off = np.array([0, len(plist)], np.uint64)
+        coefs, offs, ok = ctx.lloyd(np.array([0], np.uint32), np.array([n], np.uint32), off, plist,
+                                    pts[0:1], pts[512:513], 2)
+        o = oracle_lib.Oracle(pts, k=10)
+        ids = plist if len(plist) else np.arange(n, dtype=np.uint32)
+        oc, oo, ook = o.lloyd(ids, pts[0], pts[512], 2)
+        assert ok.all() and ook
+        np.testing.assert_array_equal(coefs[0].view(np.uint32), oc.view(np.uint32))
+        assert np.float32(offs[0]).view(np.uint32) == np.float32(oo).view(np.uint32)
+
+
 def test_device_seeded_rep_matches_counter_oracle(oracle_lib, ctx):
     """knng_run_rep (device RNG, device Lloyd, device partition, buckets) equals
     the oracle driven by the same counter RNG."""
@@ -161,6 +189,23 @@ def test_build_end_to_end_matches_oracle(oracle_lib, ctx):
     o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=4242)
     for r in range(3):
         o.rep(2, 400 if r % 2 else 200, r)
+    o.refine()
+    oids, odist = o.finalize()
+    np.testing.assert_array_equal(ids, oids)
+    np.testing.assert_array_equal(dist.view(np.uint32), odist.view(np.uint32))
+
+
+def test_config1_full_build_matches_oracle(oracle_lib, ctx):
+    """The 100k-point config at full size: 64 Gaussians (sigma 0.15, seed 0),
+    k = 100, buckets <= 256, 2 Lloyd iterations, 8 repetitions + 1
+    neighbour-of-neighbour pass.  Final ids and distance bits equal the
+    oracle's (driven by the same counter RNG)."""
+    pts = workloads.gaussian_mixture(n=100_000, d=100, clusters=64, sigma=0.15, seed=0)
+    p = default_params(reps=8, max_leaf=257, max_leaf_odd=0, lloyd_iters=2, refine=1, seed=12345)
+    ids, dist = ctx.build(pts, p, want_dists=True)
+    o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=12345)
+    for r in range(8):
+        o.rep(2, 257, r)
     o.refine()
     oids, odist = o.finalize()
     np.testing.assert_array_equal(ids, oids)

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import digest, sets_digest
+from helpers import case_points, digest, sets_digest
 from sigmod23ann_b200 import workloads
 
 
@@ -16,7 +16,7 @@ def test_oracle_matches_reference_golden(oracle_lib, golden):
     """The C++ restatement reproduces the reference's own outputs bit for bit:
     index permutation after every repetition, full set state, top-up, final ids."""
     for name, case in golden["cases"].items():
-        pts = workloads.gaussian_mixture(**case["generator"])
+        pts = case_points(case["generator"])
         o = oracle_lib.Oracle(pts, k=100, rng_mode=0, seed=12345)
         for r, (iters, leaf) in enumerate(case["reps"]):
             o.rep(iters, leaf, r)
@@ -138,7 +138,8 @@ def test_counter_mode_rep_is_deterministic(oracle_lib):
     assert sets_digest(a.sets()) == sets_digest(b.sets())
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src"), reason="needs the reference tree")
+@pytest.mark.skipif(not os.path.isdir(__import__("oracle.bindings").bindings.REFERENCE_SRC),
+                    reason="needs the reference tree")
 def test_oracle_equals_reference_on_fresh_input(oracle_lib):
     """Cross-check on an input the fixtures do not cover (only where the
     reference sources exist)."""
@@ -176,3 +177,20 @@ def test_groundtruth_and_recall():
     full = np.zeros((600, 10), np.int64)
     full[q] = gt
     assert groundtruth.recall(full, gt, q) == 1.0
+
+
+def test_lloyd_sums_follow_point_order(oracle_lib):
+    """The oracle's centroid sums run one point at a time in the Lloyd set's
+    order (src/SolutionKmeans.hpp:170-175): on data whose partial sums round,
+    the result is the one-at-a-time mean, which 256-point partials miss."""
+    from helpers import mean_in_order, rounding_points
+
+    pts = rounding_points()
+    a = pts[:512, 0]
+    assert mean_in_order(a) == np.float32(0.5)
+    assert mean_in_order(a, 256) == np.float32(0.5) + np.float32(2.0 ** -24)
+    o = oracle_lib.Oracle(pts, k=10)
+    coefs, off, ok = o.lloyd(np.arange(1024, dtype=np.uint32), pts[0], pts[512], 2)
+    assert ok
+    # c1 = (0.5, 1000, 0, ...), c2 = (0, -1000, 0.5, ...): coefs = (c1 - c2) / 2.
+    assert coefs[0] == np.float32(0.25) and coefs[2] == np.float32(-0.25) and coefs[1] == np.float32(1000.0)
