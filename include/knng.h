@@ -104,6 +104,7 @@ typedef struct knng_stats {
     double ms_refine_prep;    /* refinement: snapshot, reverse lists, scans */
     uint64_t refine_join_launches; /* join-kernel launches */
     uint64_t refine_lost;     /* points redone by the per-point pass (pool region full) */
+    uint64_t refine_passes_done; /* neighbour-of-neighbour passes run, whichever kernel ran them */
 } knng_stats;
 
 /* Fills the reference's parameters: k=100, max_leaf=200, max_leaf_odd=400,
@@ -247,14 +248,21 @@ knng_status knng_debug_tile_gram_bf16(knng_context* ctx, const float* a, uint32_
  * All pointers are device pointers on the current device.  The call is
  * asynchronous on `stream`.
  *
- * Its scratch is a fixed 4 MiB device array (32 regions of 16,384 records)
- * that every GPU loading the library keeps until the process exits; k is
- * limited to k*k <= 16,384 (k <= 128), larger k is rejected with
- * KNNG_ERR_UNSUPPORTED.  The first call on a device looks up that array's
- * device address; make it before capturing the call into a CUDA graph.  Every
- * call shares the array: calls that overlap on the GPU (different streams, or
- * devices sharing a context) race, so serialise them.  No state carries over
- * between calls. */
+ * Its scratch is a fixed 32 MiB device array (2^22 survivor records) that
+ * every GPU loading the library keeps until the process exits.  Each warp of
+ * the launch owns one region of pow2(k*k) records, so the launch width follows
+ * k: 256 warps at k = 100, 1,024 at k <= 64, 2,368 (16 per SM) at k <= 32.
+ * k must be 1..128; larger k is rejected with KNNG_ERR_UNSUPPORTED before
+ * anything runs.  Throughput: at k = 100 the pass runs about a tenth as many
+ * warps as knng_refine's per-point pass and has no tensor-core join, so on
+ * millions of points it takes many times longer than knng_refine; it is meant
+ * for callers that cannot allocate, not as the fast path.
+ * The first call in a CUDA context looks up the array's device address in
+ * that context (cudaGetSymbolAddress; later calls reuse it): make that first
+ * call before capturing the call into a CUDA graph.  Every call in one
+ * context shares the array and it keeps the last call's records: calls that
+ * overlap on the GPU in the same context (on different streams) race, so
+ * serialise them.  Nothing a call needs carries over from an earlier one. */
 knng_status knng_refine_pointwise_noalloc(const float* d_points, uint32_t n, uint32_t d, uint32_t k,
                                           uint32_t* d_snapshot, float* d_dist, uint32_t* d_ids, uint32_t* d_size,
                                           uint32_t* d_maxslot, float* d_bound, uint32_t* d_changed, void* stream);

@@ -61,6 +61,7 @@ class Stats(Structure):
         ("refine_pairs", c_uint64), ("refine_filter_pass", c_uint64), ("refine_member_skip", c_uint64),
         ("refine_exact", c_uint64), ("refine_emits", c_uint64), ("refine_overflow", c_uint64),
         ("ms_refine_prep", c_double), ("refine_join_launches", c_uint64), ("refine_lost", c_uint64),
+        ("refine_passes_done", c_uint64),
     ]
 
     def as_dict(self) -> dict:

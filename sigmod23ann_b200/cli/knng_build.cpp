@@ -80,7 +80,7 @@ int main(int argc, char** argv) {
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     std::printf("points %u  reps %llu  refine passes %llu  device ms %.1f  total ms %.1f  -> %s\n", n,
                 static_cast<unsigned long long>(st.reps_done),
-                static_cast<unsigned long long>(st.refine_join_launches), st.ms_total + st.ms_finalize, ms,
+                static_cast<unsigned long long>(st.refine_passes_done), st.ms_total + st.ms_finalize, ms,
                 out.c_str());
     return 0;
 }

@@ -467,6 +467,7 @@ void add_rep_stats(knng_stats* s, const RepStats& st) {
 
 void add_refine_stats(knng_stats* stats, const Context& c, uint64_t changed, double ms) {
     if (!stats) return;
+    stats->refine_passes_done += 1;
     stats->ms_refine += ms;
     stats->refine_changed += changed;
     stats->ms_refine_join += c.last_refine.ms_join;
@@ -607,6 +608,8 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     c->device = device;
     if (const char* r = std::getenv("KNNG_REFINE")) c->refine_mode = std::strcmp(r, "pointwise") == 0 ? 1 : 0;
     if (const char* r = std::getenv("KNNG_REFINE_SLOTS")) c->refine_slots = std::max(0, std::atoi(r));
+    if (const char* r = std::getenv("KNNG_JOIN_ORDER")) c->join_order_ids = std::strcmp(r, "id") == 0;
+    if (const char* r = std::getenv("KNNG_LEAF_CTAS")) c->leaf_ctas_per_sm = std::atoi(r) == 1 ? 1 : 2;
     if (const char* r = std::getenv("KNNG_REFINE_POOL")) c->refine_pool = std::max<long long>(0, std::atoll(r));
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {

@@ -27,10 +27,12 @@
 //     entries) and replays them.  It serves as the cross-check of the join
 //     (environment KNNG_REFINE=pointwise), as the pass for the points whose
 //     pool region filled up, and behind the allocation-free entry point.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "context.hpp"
@@ -540,7 +542,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
            const uint32_t* __restrict__ set_size, int K, uint32_t n, uint32_t slots,
            uint32_t* __restrict__ surv_count, unsigned long long* __restrict__ surv, uint4* __restrict__ pool,
            uint32_t pool_cap, uint32_t* __restrict__ pool_fill, uint8_t* __restrict__ lost,
-           uint32_t* __restrict__ error_flag, unsigned long long* __restrict__ counters) {
+           uint32_t* __restrict__ error_flag, unsigned long long* __restrict__ counters,
+           const uint32_t* __restrict__ order, uint32_t* __restrict__ work) {
     using L = JoinLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
     const JoinSmem S = join_smem(D, static_cast<uint32_t>(K));
@@ -583,7 +586,16 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     const int KS = list_stride(D, static_cast<uint32_t>(K));
     int search_top = 1;  // largest power of two <= K (branch-free lower bound)
     while (search_top * 2 <= K) search_top *= 2;
-    for (uint32_t q = blockIdx.x; q < n && healthy; q += gridDim.x) {
+    // Work: positions of `order` (the last repetition's leaf order, so that
+    // the CTAs running at the same time take neighbouring points, whose rows
+    // and lists overlap and stay in L2), handed out one at a time.
+    __shared__ uint32_t work_s[2];
+    for (uint32_t it = 0; healthy; ++it) {
+        if (tid == 0) work_s[it & 1u] = atomicAdd(work, 1u);
+        __syncthreads();
+        const uint32_t w = work_s[it & 1u];
+        if (w >= n) break;
+        const uint32_t q = order ? order[w] : w;
         const unsigned long long rb = rev_off[q], re = rev_off[q + 1];
         if (rb == re) continue;
         // Columns: the distinct ids of S(q), ascending.
@@ -1194,6 +1206,7 @@ uint64_t run_refine(Context& c) {
     auto* err = static_cast<uint32_t*>(scratch(c, "join_error", sizeof(uint32_t)));
     auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 8 * sizeof(unsigned long long)));
     auto* counters = static_cast<uint32_t*>(scratch(c, "apply_counters", 4 * sizeof(uint32_t)));
+    auto* work = static_cast<uint32_t*>(scratch(c, "join_work", sizeof(uint32_t)));
     auto* big = static_cast<uint32_t*>(scratch(c, "apply_big", static_cast<size_t>(n) * sizeof(uint32_t)));
     unsigned long long* direct =
         slots ? static_cast<unsigned long long*>(
@@ -1208,6 +1221,10 @@ uint64_t run_refine(Context& c) {
     KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
     KNNG_CUDA(cudaMemsetAsync(jc, 0, 8 * sizeof(unsigned long long), c.stream));
     KNNG_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), c.stream));
+    // Points in the leaf order of the last repetition (c.indices), unless the
+    // context was created with KNNG_JOIN_ORDER=id.
+    const uint32_t* order = c.join_order_ids ? nullptr : c.indices;
     auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
         float ms = 0.f;
         KNNG_CUDA(cudaEventElapsedTime(&ms, a, b));
@@ -1217,7 +1234,7 @@ uint64_t run_refine(Context& c) {
     KNNG_DISPATCH_D(c.d, {
         k_join<D><<<kJoinBlocks, kJoinThreads, join_bytes, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K,
                                                             n, slots, scount, direct, pool, pool_cap, pool_fill, lost,
-                                                            err, jc);
+                                                            err, jc, order, work);
     });
     ++c.launches;
     ++rec.join_launches;
@@ -1325,32 +1342,80 @@ uint64_t run_refine(Context& c) {
 // one-warp-per-point pass on buffers the caller passes in, and keeps its only
 // scratch -- each warp's survivor records -- in the fixed device array below,
 // which every GPU that loads the library holds until the process exits.
+//
+// The array is cut into one region per warp of pow2(k*k) records (a point has
+// at most k*k candidates), so the launch is as wide as the array allows for
+// the caller's k: 256 warps at k = 100, 1024 at k <= 64, up to 2,368 (16 per
+// SM) at k <= 32.
 namespace {
 
-constexpr uint32_t kNoAllocWarps = 32;                 // warps of the launch; one scratch region each
-constexpr uint32_t kNoAllocRegion = 16384;             // records per region: >= k*k for every k <= 128
-static __device__ __align__(256) unsigned long long g_noalloc_survivors[kNoAllocWarps * kNoAllocRegion];  // 4 MiB
+constexpr uint64_t kNoAllocRecords = 1ull << 22;  // 32 MiB of 8-byte survivor records
+constexpr uint32_t kNoAllocMaxWarps = 148 * 16;
+static __device__ __align__(256) unsigned long long g_noalloc_survivors[kNoAllocRecords];
 
-constexpr int kNoAllocMaxDevices = 64;
+// The device address of that array differs per CUDA context, and a context
+// handle can be reused after its context is destroyed, so the cache is keyed on
+// the context's unique id (cuCtxGetId), resolved through the runtime's driver
+// entry points (no link-time dependence on the driver library).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+struct NoAllocEntry {
+    unsigned long long ctx_id;
+    void* addr;
+};
+
 std::mutex g_noalloc_mutex;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+std::vector<NoAllocEntry> g_noalloc_cache;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
 
-// Device address of the scratch array on the current device, resolved once per
-// device (the array's name in host code is a host-side stand-in, not a device
-// address).
+cudaError_t current_context_id(unsigned long long* id) {
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void* f = nullptr;
+        void* g = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return e;
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, &q2);
+        if (e != cudaSuccess) return e;
+        if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f || !g)
+            return cudaErrorNotSupported;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(g);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return cudaErrorDeviceUninitialized;
+    return g_ctx_get_id(ctx, id) == CUDA_SUCCESS ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
+
+// Device address of the scratch array in the current context, looked up with
+// cudaGetSymbolAddress the first time a context calls (the array's name in host
+// code is a host-side stand-in, not a device address).
 cudaError_t noalloc_scratch(unsigned long long** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
+    unsigned long long id = 0;
+    cudaError_t e = current_context_id(&id);
+    if (e == cudaErrorDeviceUninitialized) {
+        // No context is current yet: the lookup below makes the device's
+        // primary context current, then its id is taken.
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_survivors);
         if (e != cudaSuccess) return e;
-        g_noalloc_addr[dev] = p;
+        e = current_context_id(&id);
     }
-    *out = static_cast<unsigned long long*>(g_noalloc_addr[dev]);
+    if (e != cudaSuccess) return e;
+    for (const NoAllocEntry& c : g_noalloc_cache) {
+        if (c.ctx_id == id) {
+            *out = static_cast<unsigned long long*>(c.addr);
+            return cudaSuccess;
+        }
+    }
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_survivors);
+    if (e != cudaSuccess) return e;
+    g_noalloc_cache.push_back({id, p});
+    *out = static_cast<unsigned long long*>(p);
     return cudaSuccess;
 }
 
@@ -1361,8 +1426,8 @@ extern "C" knng_status knng_refine_pointwise_noalloc(const float* d_points, uint
                                                      uint32_t* d_size, uint32_t* d_maxslot, float* d_bound,
                                                      uint32_t* d_changed, void* stream) {
     using namespace knng;
-    // A point has at most k*k candidates; a scratch region holds kNoAllocRegion.
-    if (k == 0 || static_cast<uint64_t>(k) * k > kNoAllocRegion) return KNNG_ERR_UNSUPPORTED;
+    // A point has at most k*k candidates; the set capacity is at most 128.
+    if (k == 0 || k > static_cast<uint32_t>(kMaxK)) return KNNG_ERR_UNSUPPORTED;
     if (!dim_supported(d)) return KNNG_ERR_UNSUPPORTED;
     if (n == 0) return KNNG_OK;
     if (!d_points || !d_snapshot || !d_dist || !d_ids || !d_size || !d_maxslot || !d_bound || !d_changed)
@@ -1373,6 +1438,12 @@ extern "C" knng_status knng_refine_pointwise_noalloc(const float* d_points, uint
         cudaGetLastError();
         return KNNG_ERR_CUDA;
     }
+    // One region of pow2(k*k) records per warp; whole blocks of kRefWarps.
+    const uint32_t region = pow2_at_least(k * k);
+    const uint64_t fit = kNoAllocRecords / region;
+    const uint32_t warps = static_cast<uint32_t>(std::min<uint64_t>(fit, kNoAllocMaxWarps)) / kRefWarps * kRefWarps;
+    const uint32_t need = (n + kRefWarps - 1) / kRefWarps * kRefWarps;
+    const uint32_t blocks = std::max<uint32_t>(1, std::min(warps, need) / kRefWarps);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int K = static_cast<int>(k);
     if (cudaMemsetAsync(d_changed, 0, sizeof(uint32_t), s) != cudaSuccess) {
@@ -1383,9 +1454,9 @@ extern "C" knng_status knng_refine_pointwise_noalloc(const float* d_points, uint
     k_snapshot<<<sblocks, kSnapWarps * kWarp, 0, s>>>(d_ids, n, K, d_snapshot);
     try {
         KNNG_DISPATCH_D(d, {
-            k_refine<D><<<kNoAllocWarps / kRefWarps, kRefWarps * kWarp, 0, s>>>(
-                d_snapshot, d_points, static_cast<int>(d), d_dist, d_ids, d_size, d_maxslot, d_bound, K, n, nullptr,
-                scratch_keys, kNoAllocRegion, d_changed);
+            k_refine<D><<<blocks, kRefWarps * kWarp, 0, s>>>(d_snapshot, d_points, static_cast<int>(d), d_dist,
+                                                             d_ids, d_size, d_maxslot, d_bound, K, n, nullptr,
+                                                             scratch_keys, region, d_changed);
         });
     } catch (const Error& e) {
         return e.status;

@@ -44,10 +44,26 @@ def test_status_strings(knng_lib):
     assert knng_lib.knng_status_string(0) == b"ok"
 
 
-def test_struct_layouts_match_header():
-    # knng_params: 8 x uint32 + uint64; knng_stats: 10 doubles + 19 uint64.
+def test_struct_layouts_match_header(tmp_path):
+    """Sizes and field offsets of the ctypes mirrors equal the C header's (a C
+    program compiled against include/knng.h prints them)."""
+    import subprocess
+
     assert ctypes.sizeof(api.Params) == 40
-    assert ctypes.sizeof(api.Stats) == 10 * 8 + 19 * 8
+    assert ctypes.sizeof(api.Stats) == 10 * 8 + 20 * 8
+    checks = [("knng_stats", name) for name, _ in api.Stats._fields_] + \
+             [("knng_params", name) for name, _ in api.Params._fields_]
+    src = tmp_path / "layout.c"
+    body = "".join(f'    printf("%zu\\n", offsetof({t}, {f}));\n' for t, f in checks)
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "knng.h"\nint main(void) {\n'
+                   '    printf("%zu\\n%zu\\n", sizeof(knng_stats), sizeof(knng_params));\n' + body +
+                   "    return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [ctypes.sizeof(api.Stats), ctypes.sizeof(api.Params)] + \
+           [getattr(api.Stats if t == "knng_stats" else api.Params, f).offset for t, f in checks]
+    assert got == want
 
 
 def test_create_without_device_reports_no_device(knng_lib):

@@ -293,15 +293,19 @@ def refine_case(knng_lib):
     return pts, s0, changed, s1
 
 
-@pytest.mark.parametrize("slots,pool", [(None, None), ("16", "1000000"), ("0", "1000000"), ("16", "64"), ("0", "0")])
-def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, pool):
+@pytest.mark.parametrize("slots,pool,order", [(None, None, None), (None, None, "id"), ("16", "1000000", None),
+                                              ("0", "1000000", None), ("16", "64", None), ("0", "0", None)])
+def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, pool, order):
     """The tensor-core local join and the one-warp-per-point pass leave
     identical sets, however the join's survivors are stored: per-point slots
     sized from the budget, small or no slots with the rest pooled, or pool
-    regions so small that points lose records and are redone point by point."""
+    regions so small that points lose records and are redone point by point;
+    and whichever order the join takes the points in (leaf order or id order)."""
     from sigmod23ann_b200.api import Stats
 
     pts, s0, changed, s1 = refine_case
+    if order is not None:
+        monkeypatch.setenv("KNNG_JOIN_ORDER", order)
     if slots is not None:
         monkeypatch.setenv("KNNG_REFINE_SLOTS", slots)
     if pool is not None:
@@ -311,6 +315,10 @@ def test_refine_join_equals_pointwise(refine_case, monkeypatch, slots, pool):
         a.load_points(pts)
         a.reset_sets(100)
         a.set_sets(s0)
+        # The join walks the points in the order the context's index
+        # permutation gives (a repetition's leaf order); any permutation must
+        # give the same sets.
+        a.set_indices(np.random.default_rng(11).permutation(len(pts)).astype(np.uint32))
         ch = a.refine(st)
         sa = a.sets()
     assert ch == changed
@@ -375,12 +383,12 @@ def test_timed_build_equals_fixed_count_build(knng_lib):
     with KnngContext(0) as ctx:
         ids = ctx.build_timed(pts, build_ms=400, refine_ms=2000, params=params, stats=st)
         assert st.reps_done >= 1
-        fixed = ctx.build(pts, default_params(reps=int(st.reps_done), refine=int(st.refine_join_launches),
+        fixed = ctx.build(pts, default_params(reps=int(st.reps_done), refine=int(st.refine_passes_done),
                                               max_leaf=200, max_leaf_odd=400, lloyd_iters=1, seed=3))
         assert np.array_equal(ids, fixed)
         one = Stats()
         ctx.build_timed(pts, build_ms=1, refine_ms=0, params=params, stats=one)
-        assert one.reps_done == 1 and one.refine_join_launches == 0
+        assert one.reps_done == 1 and one.refine_passes_done == 0
 
 
 def test_sets_snapshot_and_resume(knng_lib, tmp_path):

@@ -44,7 +44,7 @@ def _run_noalloc(lib, pts: np.ndarray, sets: dict, k: int):
     return out, int(changed.cpu().numpy()[0])
 
 
-def test_noalloc_pass_matches_knng_refine_on_two_calls_in_a_row():
+def test_noalloc_pass_matches_knng_refine_on_two_calls_in_a_row(oracle_lib):
     lib = load_library()
     # Two calls in a row on different inputs: the shared scratch array keeps the
     # first call's records, which must not leak into the second.
@@ -60,11 +60,16 @@ def test_noalloc_pass_matches_knng_refine_on_two_calls_in_a_row():
         assert changed == changed_ref
         # Bit-exact, the tolerance of every set comparison in this suite.
         assert_sets_equal(after, after_ref, f"allocation-free pass, seed {seed}")
+        # and the oracle's neighbour-of-neighbour pass from the same sets.
+        o = oracle_lib.Oracle(pts, k=k)
+        o.set_sets(before)
+        assert o.refine() == changed
+        assert_sets_equal(after, o.sets(), f"allocation-free pass vs oracle, seed {seed}")
 
 
 def test_noalloc_rejects_k_beyond_its_scratch():
     lib = load_library()
-    # k*k must fit one 16,384-record scratch region: k = 129 is refused
-    # before anything runs (null buffers are never touched).
+    # Sets hold at most 128 neighbours: k = 129 is refused before anything
+    # runs (null buffers are never touched).
     status = lib.knng_refine_pointwise_noalloc(None, 10, 100, 129, None, None, None, None, None, None, None, None)
     assert STATUS_NAMES[status] == "KNNG_ERR_UNSUPPORTED"
