@@ -71,8 +71,8 @@ def parse_args(argv=None):
     ap.add_argument("--serving", action="store_true", help="measure only the serving stream")
     ap.add_argument("--batched", action="store_true", help="measure only the batched form (4,096 sets, 5 waves)")
     ap.add_argument("--bf16", action="store_true",
-                    help="time the precision form (BF16 estimates + FP32 re-rank, buckets <= 512) instead")
-    ap.add_argument("--max-leaf", type=int, default=0, help="leaf test bound (0: 1025, or 513 with --bf16)")
+                    help="time the precision form (BF16 estimates + FP32 re-rank) instead")
+    ap.add_argument("--max-leaf", type=int, default=0, help="leaf test bound (0: 1025, buckets of at most 1024)")
     ap.add_argument("--precision", action="store_true",
                     help="measure only the precision form against the FP32 form (100k-point config)")
     ap.add_argument("--batched-waves", type=int, default=5, help="waves of the batched form to run (of 5)")
@@ -598,7 +598,7 @@ def run_ours(args):
     n = args.n
     from sigmod23ann_b200.api import PRECISION_BF16_RERANK, PRECISION_FP32
 
-    max_leaf = args.max_leaf or (513 if args.bf16 else MAX_LEAF)
+    max_leaf = args.max_leaf or MAX_LEAF
     params = default_params(k=K, max_leaf=max_leaf, max_leaf_odd=0, lloyd_iters=LLOYD_ITERS, reps=args.reps,
                             refine=args.refine, seed=SEED,
                             precision=PRECISION_BF16_RERANK if args.bf16 else PRECISION_FP32)

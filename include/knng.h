@@ -220,9 +220,9 @@ knng_status knng_finalize(knng_context* ctx, uint32_t* out_ids, float* out_dists
 
 /* -------------------------------------------------------------- diagnostics
  * No counterpart in the reference.  Runs one 128 x 128 tensor-core tile
- * (tcgen05.mma kind::tf32, the tile the refinement pass filters with) on
+ * (tcgen05.mma kind::f16, the tile the refinement pass filters with) on
  * a (m x d) and b (n x d), m, n <= 128, writing out[i*n + j] = a_i . b_j
- * with TF32 operands and FP32 accumulation. */
+ * with both operands rounded to FP16 and FP32 accumulation. */
 knng_status knng_debug_tile_gram(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n,
                                  uint32_t d, float* out);
 
@@ -231,6 +231,14 @@ knng_status knng_debug_tile_gram(knng_context* ctx, const float* a, uint32_t m, 
  * the reference. */
 knng_status knng_debug_tile_gram_bf16(knng_context* ctx, const float* a, uint32_t m, const float* b, uint32_t n,
                                       uint32_t d, float* out);
+
+/* Poll limit of the waits the tree-construction and refinement kernels make
+ * on their own bulk copies and tensor-core operations, on the context's device
+ * (default 2^26 polls).  After a wait runs out the kernel records the failure,
+ * drains its copies in flight with the default limit and returns; the call
+ * reports KNNG_ERR_CUDA and the context stays usable.  A test sets a limit of
+ * 0 to make every such wait run out.  No counterpart in the reference. */
+knng_status knng_debug_set_wait_limit(knng_context* ctx, uint32_t polls);
 
 /* ------------------------------------------------------ allocation-free pass
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -35,7 +35,8 @@ EXPORTED = [
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
     "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
-    "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_refine_pointwise_noalloc", "knng_build_batch",
+    "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_debug_set_wait_limit", "knng_refine_pointwise_noalloc",
+    "knng_build_batch",
     "knng_build_timed", "knng_save_sets", "knng_load_sets", "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
     "knng_server_job_error", "knng_server_release", "knng_server_destroy",
 ]
@@ -118,6 +119,7 @@ def load_library(path: str = LIB_PATH):
         "knng_set_sets": (c_int, [P, P, P, P, P, P]),
         "knng_finalize": (c_int, [P, P, P]),
         "knng_debug_tile_gram": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
+        "knng_debug_set_wait_limit": (c_int, [P, c_uint32]),
         "knng_debug_tile_gram_bf16": (c_int, [P, P, c_uint32, P, c_uint32, c_uint32, P]),
         "knng_refine_pointwise_noalloc": (c_int, [P, c_uint32, c_uint32, c_uint32, P, P, P, P, P, P, P, P]),
         "knng_save_sets": (c_int, [P, c_char_p]),
@@ -383,8 +385,13 @@ class KnngContext:
         return (ids, dists) if want_dists else ids
 
 
+def debug_set_wait_limit(ctx: "KnngContext", polls: int) -> None:
+    """Poll limit of the kernels' bounded waits on the context's device (diagnostic; default 2**26)."""
+    ctx._check(ctx._lib.knng_debug_set_wait_limit(ctx._h, polls))
+
+
 def debug_tile_gram(ctx: "KnngContext", a: np.ndarray, b: np.ndarray) -> np.ndarray:
-    """a . b^T through one tcgen05 TF32 tile (diagnostic)."""
+    """a . b^T through one tcgen05 tile, FP16 operands, FP32 accumulation (diagnostic)."""
     a = _f32(a)
     b = _f32(b)
     out = np.zeros((a.shape[0], b.shape[0]), np.float32)

@@ -492,8 +492,8 @@ void validate_params(const knng_params* p) {
     if (p->max_leaf > 4097 || p->max_leaf_odd > 4097) fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be <= 4097");
     if (p->precision != KNNG_PRECISION_FP32 && p->precision != KNNG_PRECISION_BF16_RERANK)
         fail(KNNG_ERR_UNSUPPORTED, "unknown precision");
-    if (p->precision == KNNG_PRECISION_BF16_RERANK && (p->max_leaf > 513 || p->max_leaf_odd > 513))
-        fail(KNNG_ERR_UNSUPPORTED, "the BF16 form takes buckets of at most 512 points (max_leaf <= 513)");
+    if (p->precision == KNNG_PRECISION_BF16_RERANK && (p->max_leaf > 1025 || p->max_leaf_odd > 1025))
+        fail(KNNG_ERR_UNSUPPORTED, "the BF16 form takes buckets of at most 1024 points (max_leaf <= 1025)");
 }
 
 // All repetitions, then all refinement passes.  With build_ms > 0 (the
@@ -1057,6 +1057,13 @@ knng_status knng_debug_tile_gram_bf16(knng_context* ctx, const float* a, uint32_
         float* dout = static_cast<float*>(knng::scratch(c, "dbg_out", static_cast<size_t>(m) * n * sizeof(float)));
         knng::run_tile_gram_bf16(c, d, da, m, db, n, dout);
         knng::download(c, out, dout, static_cast<size_t>(m) * n);
+    });
+}
+
+knng_status knng_debug_set_wait_limit(knng_context* ctx, uint32_t polls) {
+    return knng::guarded(ctx, [&](Context&) {
+        knng::set_split_wait_limit(polls);
+        knng::set_refine_wait_limit(polls);
     });
 }
 

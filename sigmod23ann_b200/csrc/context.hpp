@@ -200,6 +200,9 @@ void launch_leaves_bf16(Context& c, uint32_t count, const uint32_t* d_starts, co
 // One 128 x 128 BF16 tile a(m x d) . b(n x d)^T into d_out (m x n), m, n <= 128.
 void run_tile_gram_bf16(Context& c, uint32_t d, const float* d_a, uint32_t m, const float* d_b, uint32_t n,
                         float* d_out);
+// Poll limits of the kernels' bounded waits (split.cu, refine.cu).
+void set_split_wait_limit(uint32_t polls);
+void set_refine_wait_limit(uint32_t polls);
 // refine.cu
 uint64_t run_refine(Context& c);
 // One tensor-core tile a(m x d) . b(n x d)^T into d_out (m x n), m, n <= 128.

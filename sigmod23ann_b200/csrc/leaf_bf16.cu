@@ -7,18 +7,19 @@
 //   1. the bucket's rows, centred on its first point, are rounded to BF16 and
 //      multiplied on the tensor cores (tcgen05.mma kind::f16, FP32
 //      accumulation): approx(i, j) = |x_i'|^2 + |x_j'|^2 - 2 bf16(x_i').bf16(x_j'),
-//      with the norms of the FP32 centred rows; a block of 128 rows against the
-//      whole bucket lands in TMEM (at most 512 columns);
-//   2. one thread per row finds the 128th smallest estimate by bisection over
-//      its bit pattern (non-negative floats order like their bits) and keeps
-//      the candidates at or below it, ties in bucket order, 128 in all;
+//      with the norms of the FP32 centred rows; a block of 128 rows against a
+//      tile of 128 columns at a time lands in TMEM;
+//   2. one thread per row keeps the 128 smallest (estimate, bucket position)
+//      keys seen so far in a max-heap in shared memory, reading every TMEM
+//      column once: the kept set is every candidate whose estimate is below
+//      the 128th smallest, then ties in bucket order;
 //   3. each kept candidate gets the exact FP32 distance in the reference's
 //      order and is offered to the point's set in bucket position order (the
 //      order of the FP32 form), through the same warp-resident set update.
 //
-// Buckets of at most 512 points (max_leaf <= 513).  The result differs from the
-// FP32 form only where a candidate outside a point's 128 best estimates would
-// have entered its set.
+// Buckets of at most 1024 points (max_leaf <= 1025).  The result differs from
+// the FP32 form only where a candidate outside a point's 128 best estimates
+// would have entered its set.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -36,23 +37,50 @@ constexpr int kBfThreads = 256;
 constexpr int kBfRows = 128;   // MMA M: rows per block
 constexpr int kBfCols = 128;   // MMA N: columns per tile
 constexpr int kKeep = 128;     // candidates re-ranked per point
-constexpr int kBfMaxBucket = 512;
+constexpr int kBfMaxBucket = 1024;
 
 template <int D>
 struct BfLayout {
     static constexpr int KP = (D + 15) / 16 * 16;  // K padded to the MMA step (16 BF16)
     static constexpr int CH = KP / 8;              // 16-byte chunks per row
     static constexpr uint32_t tile_bytes = kBfRows * KP * 2;
-    // A tile, B tile, norms of every bucket row, the centre, bucket ids, and
-    // every row's kept candidates (bucket positions, ascending)
+    // A tile, B tile, every block row's heap of kept keys ([slot][row]),
+    // norms of every bucket row, the centre, bucket ids.  Once a row block's
+    // selection is done its kept bucket positions (ascending) take the tiles'
+    // space.
     static constexpr uint32_t a = 0;
     static constexpr uint32_t b = a + tile_bytes;
-    static constexpr uint32_t norms = b + tile_bytes;
+    static constexpr uint32_t keep = a;
+    static constexpr uint32_t heap = b + tile_bytes;
+    static constexpr uint32_t norms = heap + kKeep * kBfRows * 8;
     static constexpr uint32_t centre = norms + kBfMaxBucket * 4;
     static constexpr uint32_t ids = centre + (D + 3) / 4 * 16;
-    static constexpr uint32_t keep = ids + kBfMaxBucket * 4;
-    static constexpr uint32_t bytes = keep + kBfRows * kKeep * 2;
+    static constexpr uint32_t bytes = ids + kBfMaxBucket * 4;
+    static_assert(kBfRows * kKeep * 2 <= 2 * tile_bytes, "kept positions fit the tiles' space");
 };
+
+// Max-heap of `n` keys in column `r` of a [slot][kBfRows] array: restores the
+// heap order below slot i.
+__device__ __forceinline__ void heap_sift_down(unsigned long long* __restrict__ h, uint32_t r, uint32_t n, uint32_t i) {
+    const unsigned long long key = h[i * kBfRows + r];
+    for (;;) {
+        const uint32_t l = 2 * i + 1;
+        if (l >= n) break;
+        uint32_t c = l;
+        unsigned long long cv = h[l * kBfRows + r];
+        if (l + 1 < n) {
+            const unsigned long long rv = h[(l + 1) * kBfRows + r];
+            if (rv > cv) {
+                c = l + 1;
+                cv = rv;
+            }
+        }
+        if (cv <= key) break;
+        h[i * kBfRows + r] = cv;
+        i = c;
+    }
+    h[i * kBfRows + r] = key;
+}
 
 // Rows ids[r] (r < count) minus `centre`, rounded to BF16, into a chunk-major
 // tile of 128 rows (rows past `count` and dims past D are zero).  Threads with
@@ -104,15 +132,16 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     k_leaf_bf16(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,
                 const uint32_t* __restrict__ idx, const float* __restrict__ pts, int ld, float* __restrict__ set_dist,
                 uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
-                float* __restrict__ set_bound, int K, uint32_t tmem_cols, uint32_t* __restrict__ error_flag) {
+                float* __restrict__ set_bound, int K, uint32_t* __restrict__ error_flag) {
     using L = BfLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* A = smem + L::a;
     unsigned char* B = smem + L::b;
+    unsigned long long* heap = reinterpret_cast<unsigned long long*>(smem + L::heap);
+    uint16_t* keep = reinterpret_cast<uint16_t*>(smem + L::keep);
     float* norms = reinterpret_cast<float*>(smem + L::norms);
     float* centre = reinterpret_cast<float*>(smem + L::centre);
     uint32_t* ids = reinterpret_cast<uint32_t*>(smem + L::ids);
-    uint16_t* keep = reinterpret_cast<uint16_t*>(smem + L::keep);
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     const uint32_t s0 = starts[blockIdx.x];
@@ -120,7 +149,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     if (b < 2) return;
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
     for (uint32_t t = tid; t < b; t += kBfThreads) ids[t] = idx[s0 + t];
-    if (warp == 0) tc::tmem_alloc(&tmem_slot, tmem_cols);
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, kBfCols);
     if (tid == 0) {
         tc::mbar_init(&mbar, 1);
         tc::fence_barrier_init();
@@ -135,112 +164,96 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     uint32_t phase = 0;
     bool healthy = true;
     const uint32_t idesc = tc::idesc_bf16(kBfRows, kBfCols);
+    const bool keep_all = b - 1 <= static_cast<uint32_t>(kKeep);
     for (uint32_t rb = 0; rb < b && healthy; rb += kBfRows) {
         const uint32_t cnt = min(static_cast<uint32_t>(kBfRows), b - rb);
         stage_bf16<D>(A, ids + rb, cnt, pts, ld, centre);
-        // The bucket's columns, one 128-column tile at a time, into TMEM
-        // columns [cb, cb + 128).
-        for (uint32_t cb = 0; cb < b; cb += kBfCols) {
+        // Selection state of the row this thread owns (warps 0-3: TMEM lane r).
+        const uint32_t r = static_cast<uint32_t>(warp * kWarp + lane);
+        const uint32_t i = rb + r;  // bucket position of the row's point
+        uint32_t n_in = 0;
+        // The bucket's columns, one 128-column tile at a time.
+        for (uint32_t cb = 0; cb < b && !keep_all; cb += kBfCols) {
             stage_bf16<D>(B, ids + cb, min(static_cast<uint32_t>(kBfCols), b - cb), pts, ld, centre);
             tc::fence_proxy_async();
             tc::fence_before_sync();
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after_sync();
-                tc::issue_tile_bf16(tmem + cb, tc::smem_u32(A), tc::smem_u32(B), kBfRows, kBfCols, L::KP, idesc);
+                tc::issue_tile_16bit(tmem, tc::smem_u32(A), tc::smem_u32(B), kBfRows, kBfCols, L::KP, idesc);
                 tc::mma_commit(&mbar);
             }
             const bool done = tc::mbar_wait(&mbar, phase);
             phase ^= 1u;
             if (__syncthreads_or(!done)) {
                 if (tid == 0) atomicExch(error_flag, 1u);
+                tc::mbar_wait(&mbar, phase ^ 1u);
                 healthy = false;
                 break;
             }
             tc::fence_after_sync();
-        }
-        if (!healthy) break;
-        // Selection: thread r of the first four warps owns row r (its TMEM lane).
-        if (warp < 4) {
-            const uint32_t r = static_cast<uint32_t>(warp * kWarp + lane);
-            const uint32_t i = rb + r;  // bucket position of the row's point
-            const float na = r < cnt ? norms[i] : 0.f;
-            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * kWarp) << 16);
-            // Estimate bits of column j (+inf for the point itself and past b).
-            auto bits_of = [&](uint32_t j, float g) -> uint32_t {
-                if (j >= b || j == i) return 0x7F800000u;
-                const float v = fmaxf(0.f, na + norms[j] - 2.0f * g);
-                return __float_as_uint(v);
-            };
-            uint32_t thr = 0x7F800000u;  // keep every column below this, and ties in order
-            if (b - 1 > static_cast<uint32_t>(kKeep)) {
-                // Smallest bit pattern with at least 128 estimates at or below
-                // it; 31 halvings cover [0, +inf] (a fixed count: the TMEM
-                // loads are warp-collective).
-                uint32_t lo = 0, hi = 0x7F800000u;
-                for (int it = 0; it < 31; ++it) {
-                    const uint32_t mid = lo + (hi - lo) / 2;
-                    uint32_t c = 0;
-                    for (uint32_t j0 = 0; j0 < b; j0 += 16) {
-                        float g[16];
-                        tc::tmem_ld16(taddr + j0, g);
-                        tc::tmem_wait_ld();
-#pragma unroll
-                        for (int u = 0; u < 16; ++u) c += bits_of(j0 + u, g[u]) <= mid ? 1u : 0u;
-                    }
-                    if (c >= static_cast<uint32_t>(kKeep)) hi = mid; else lo = mid + 1;
-                }
-                thr = lo;
-            }
-            // Kept candidates in column order: every estimate below thr, then
-            // ties at thr until 128.
-            uint32_t below = 0;
-            if (b - 1 > static_cast<uint32_t>(kKeep)) {
-                for (uint32_t j0 = 0; j0 < b; j0 += 16) {
+            if (warp < 4) {
+                const float na = r < cnt ? norms[i] : 0.f;
+                const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * kWarp) << 16);
+                for (uint32_t j0 = 0; j0 < kBfCols && cb + j0 < b; j0 += 16) {  // warp-uniform
                     float g[16];
                     tc::tmem_ld16(taddr + j0, g);
                     tc::tmem_wait_ld();
-#pragma unroll
-                    for (int u = 0; u < 16; ++u) below += bits_of(j0 + u, g[u]) < thr ? 1u : 0u;
+                    if (r >= cnt) continue;
+#pragma unroll 4
+                    for (int u = 0; u < 16; ++u) {
+                        const uint32_t j = cb + j0 + u;
+                        if (j >= b || j == i) continue;
+                        const float v = fmaxf(0.f, na + norms[j] - 2.0f * g[u]);
+                        const unsigned long long key =
+                            (static_cast<unsigned long long>(__float_as_uint(v)) << 32) | j;
+                        if (n_in < static_cast<uint32_t>(kKeep)) {
+                            heap[n_in * kBfRows + r] = key;
+                            if (++n_in == static_cast<uint32_t>(kKeep))
+                                for (int h = kKeep / 2 - 1; h >= 0; --h) heap_sift_down(heap, r, kKeep, h);
+                        } else if (key < heap[r]) {
+                            heap[r] = key;
+                            heap_sift_down(heap, r, kKeep, 0);
+                        }
+                    }
                 }
             }
-            uint32_t ties_left = static_cast<uint32_t>(kKeep) - min(below, static_cast<uint32_t>(kKeep));
-            uint32_t n_keep = 0;
-            uint16_t* mine = keep + r * kKeep;
-            for (uint32_t j0 = 0; j0 < b; j0 += 16) {
-                float g[16];
-                tc::tmem_ld16(taddr + j0, g);
-                tc::tmem_wait_ld();
-#pragma unroll
-                for (int u = 0; u < 16; ++u) {
-                    const uint32_t j = j0 + u;
-                    const uint32_t v = bits_of(j, g[u]);
-                    bool take;
-                    if (b - 1 <= static_cast<uint32_t>(kKeep))
-                        take = j < b && j != i;
-                    else if (v < thr)
-                        take = true;
-                    else if (v == thr && ties_left > 0 && j < b && j != i) {
-                        take = true;
-                        --ties_left;
-                    } else
-                        take = false;
-                    if (take && r < cnt && n_keep < static_cast<uint32_t>(kKeep)) mine[n_keep++] = static_cast<uint16_t>(j);
-                }
-            }
-            for (uint32_t t = n_keep; t < static_cast<uint32_t>(kKeep); ++t) mine[t] = 0xFFFFu;
+            tc::fence_before_sync();
+            __syncthreads();
         }
-        tc::fence_before_sync();
+        if (!healthy) break;
+        // Kept bucket positions of each row, ascending: every other member
+        // when the bucket has at most 129 points, else the heap's.
+        if (warp < 4 && r < cnt) {
+            uint16_t* mine = keep + r * kKeep;
+            uint32_t nk = 0;
+            if (keep_all) {
+                for (uint32_t j = 0; j < b; ++j)
+                    if (j != i) mine[nk++] = static_cast<uint16_t>(j);
+            } else {
+                for (uint32_t h = 0; h < n_in; ++h) mine[nk++] = static_cast<uint16_t>(heap[h * kBfRows + r] & 0xFFFFu);
+                for (uint32_t a2 = 1; a2 < nk; ++a2) {  // insertion sort of at most 128 positions
+                    const uint16_t v = mine[a2];
+                    uint32_t z = a2;
+                    while (z > 0 && mine[z - 1] > v) {
+                        mine[z] = mine[z - 1];
+                        --z;
+                    }
+                    mine[z] = v;
+                }
+            }
+            for (uint32_t t = nk; t < static_cast<uint32_t>(kKeep); ++t) mine[t] = 0xFFFFu;
+        }
         __syncthreads();
         // Offers: warp w takes rows w, w + 8, ...; lanes take 32 kept
         // candidates at a time, in bucket order.
-        for (uint32_t r = static_cast<uint32_t>(warp); r < cnt; r += kBfThreads / kWarp) {
-            const uint32_t p = ids[rb + r];
+        for (uint32_t rr = static_cast<uint32_t>(warp); rr < cnt; rr += kBfThreads / kWarp) {
+            const uint32_t p = ids[rb + rr];
             WarpSet s;
             set_load(s, set_dist, set_id, set_size, set_maxslot, set_bound, p, K, lane);
             const float4* prow = reinterpret_cast<const float4*>(pts + static_cast<size_t>(p) * ld);
             for (int g0 = 0; g0 < kKeep; g0 += kWarp) {
-                const uint16_t j = keep[r * kKeep + g0 + lane];
+                const uint16_t j = keep[rr * kKeep + g0 + lane];
                 const bool valid = j != 0xFFFFu;
                 const uint32_t cand = valid ? ids[j] : 0u;
                 float d = 0.f;
@@ -257,7 +270,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, tmem_cols);
+        tc::tmem_dealloc(tmem, kBfCols);
     }
 }
 
@@ -294,7 +307,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     __syncthreads();
     if (tid == 0) {
         tc::fence_after_sync();
-        tc::issue_tile_bf16(tmem, tc::smem_u32(A), tc::smem_u32(B), kBfRows, kBfCols, L::KP,
+        tc::issue_tile_16bit(tmem, tc::smem_u32(A), tc::smem_u32(B), kBfRows, kBfCols, L::KP,
                             tc::idesc_bf16(kBfRows, kBfCols));
         tc::mma_commit(&mbar);
     }
@@ -336,35 +349,30 @@ void run_tile_gram_bf16(Context& c, uint32_t d, const float* d_a, uint32_t m, co
     KNNG_CUDA(cudaGetLastError());
     uint32_t h = 0;
     download(c, &h, err, 1);
-    if (h) fail(KNNG_ERR_CUDA, "BF16 tile: the MMA completion wait timed out");
+    if (h) fail(KNNG_ERR_CUDA, "BF16 tile: the MMA completion wait gave up");
 }
 
 void launch_leaves_bf16(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
                         uint32_t max_bucket) {
     if (count == 0) return;
     if (max_bucket > static_cast<uint32_t>(kBfMaxBucket))
-        fail(KNNG_ERR_INVALID_ARGUMENT, "the BF16 bucket pass takes buckets of at most 512 points");
+        fail(KNNG_ERR_INVALID_ARGUMENT, "the BF16 bucket pass takes buckets of at most 1024 points");
     auto* err = static_cast<uint32_t*>(scratch(c, "bf16_error", sizeof(uint32_t)));
     KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
-    // TMEM for a whole row of the bucket: 256 columns up to 256 points (two
-    // CTAs per SM), 512 above (one CTA per SM: the shared memory asked for
-    // keeps a second one off the SM, so no CTA waits for TMEM).
-    const uint32_t tmem_cols = max_bucket <= 256 ? 256u : 512u;
+    // One CTA per SM (the heaps take most of the shared memory), 128 TMEM
+    // columns each.
     KNNG_DISPATCH_D(c.d, {
-        using L = BfLayout<D>;
-        uint32_t smem = L::bytes;
-        if (tmem_cols == 512u) smem = std::max<uint32_t>(smem, 120u * 1024u);
         auto kern = k_leaf_bf16<D>;
         allow_max_smem(c, kern);
-        kern<<<count, kBfThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist, c.set_id,
-                                                    c.set_size, c.set_maxslot, c.set_bound, static_cast<int>(c.k),
-                                                    tmem_cols, err);
+        kern<<<count, kBfThreads, BfLayout<D>::bytes, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld,
+                                                                  c.set_dist, c.set_id, c.set_size, c.set_maxslot,
+                                                                  c.set_bound, static_cast<int>(c.k), err);
     });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     uint32_t h = 0;
     download(c, &h, err, 1);
-    if (h) fail(KNNG_ERR_CUDA, "BF16 bucket pass: the MMA completion wait timed out");
+    if (h) fail(KNNG_ERR_CUDA, "BF16 bucket pass: the MMA completion wait gave up");
 }
 
 }  // namespace knng

@@ -16,8 +16,8 @@
 // Two ways to collect the survivors, with the same result:
 //   * the local join (k_join, the default): per point q, the rows R(q) (points
 //     whose list holds q) against the columns S(q) (q's list) as one block; a
-//     tcgen05 TF32 tile of centred dot products rejects the pairs that provably
-//     cannot beat bound(p), members of S(p) are dropped, the rest get the exact
+//     tcgen05 tile of centred dot products (FP16 operands, FP32 accumulation)
+//     rejects the pairs that provably cannot beat bound(p), members of S(p) are dropped, the rest get the exact
 //     FP32 distance; survivors go to per-point slots, then to the CTA's pool
 //     region (k_excess_counts / k_pool_scatter turn the pool into per-point
 //     lists), and one k_apply launch sorts and replays every point's survivors;
@@ -28,6 +28,7 @@
 //     (environment KNNG_REFINE=pointwise), as the pass for the points whose
 //     pool region filled up, and behind the allocation-free entry point.
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -177,14 +178,15 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
 // one row per (p, candidate), and its dot products run on the tensor cores:
 //
 //   1. k_rev_count / scan / k_rev_fill   R(q) as a CSR (counting sort)
-//   2. k_join     per q: S(q) rows and 128-point chunks of R(q) rows, centred
-//                 on q, staged as TF32 tiles; one tcgen05 128x128 tile gives
-//                 approximate squared distances with a proven error bound, so
-//                 a pair is dropped only when its exact distance is certainly
-//                 >= bound(p).  Survivors are checked against S(p) (binary
-//                 search in shared memory: members are always rejected by the
-//                 set update), get the exact FP32 distance in the reference's
-//                 order, and when it beats bound(p) are appended to p's
+//   2. k_join     per q: S(q) rows and 128-point chunks of R(q) rows, bulk-
+//                 copied into shared memory once, centred on q into FP16
+//                 tiles; one tcgen05 128 x 128 tile gives approximate squared
+//                 distances with a proven error bound, so a pair is dropped
+//                 only when its exact distance is certainly >= bound(p).
+//                 Survivors are checked against S(p) (binary search in shared
+//                 memory: members are always rejected by the set update), get
+//                 the exact FP32 distance in the reference's order from the
+//                 staged rows, and when it beats bound(p) are appended to p's
 //                 survivor slots.
 //   3. k_apply    per p: survivors sorted by id, duplicates dropped, replayed
 //                 through the sequential set update in ascending id order --
@@ -298,56 +300,61 @@ __global__ void k_rev_fill(const uint32_t* __restrict__ snap, uint32_t n, int K,
     }
 }
 
-constexpr int kJoinThreads = 256;
-constexpr int kTile = 128;      // MMA M (rows of R(q) per chunk)
+constexpr int kJoinThreads = 512;
+constexpr int kJoinWarps = kJoinThreads / kWarp;  // 16
+constexpr int kTile = 128;                        // MMA M: rows of R(q) per chunk
+constexpr int kGroupCols = 32;                    // columns one thread filters (4 groups of 32)
 
+// FP16 operand tiles, chunk-major: K padded to the MMA step of 16, a row held
+// as KP / 8 chunks of 16 bytes (8 halves).
 template <int D>
 struct JoinLayout {
-    static constexpr int KP = (D + 7) / 8 * 8;  // K padded to the MMA step (8 tf32)
-    static constexpr int CH = KP / 4;           // 16-byte chunks per row
-    static constexpr size_t tile_bytes = static_cast<size_t>(kTile) * KP * 4;
-    static_assert(tile_bytes >= static_cast<size_t>(kTile) * D * 4, "original rows must fit in a tile");
+    static constexpr int KP = (D + 15) / 16 * 16;
+    static constexpr int CH = KP / 8;
 };
 
 // Columns of the B tile: S(q) has at most k distinct ids; the MMA takes N in
 // steps of 16.
 __host__ __device__ constexpr uint32_t join_cols(uint32_t K) { return K <= 16 ? 16u : (K + 15) / 16 * 16; }
 
-// Dynamic shared memory of k_join (byte offsets).  A' (128 x KP) and B'
-// (NB x KP) hold the centred TF32 tiles; once the MMA has consumed them, the
-// rows' sorted lists S(p), then the original FP32 rows (row-major, D
-// floats).  `x` holds the per-thread pair masks and their prefix sums.
+// Row stride (in ids) of the staged sorted lists: k when k is a multiple of 4
+// (each list one 16-byte aligned bulk copy), else odd (searches by different
+// rows spread over the banks).
+__host__ __device__ constexpr uint32_t list_stride(uint32_t K) { return (K & 3u) == 0 ? K : (K | 1u); }
+
+// Dynamic shared memory of k_join (byte offsets).  rows_a / rows_b: the
+// original FP32 rows of R(q) (a chunk of up to 128) and of S(q), row-major;
+// they feed both the centred FP16 tiles and the exact distances.  tiles: the
+// A' and B' operand tiles, and once the MMA has read them the lists S(p) of
+// the chunk's rows.  x: per-thread pair masks, member masks, prefix sums.
 struct JoinSmem {
-    uint32_t a, b, norm_a, norm_b, bnd, pid, cid, fullrow, centre, x, bytes;
+    uint32_t rows_a, rows_b, tiles, tile_b, norm_a, norm_b, rt_a, rt_b, bnd, pid, cid, fullrow, centre, x, bytes;
 };
 
 __host__ __device__ inline JoinSmem join_smem(int D, uint32_t K) {
-    const uint32_t KP = (D + 7) / 8 * 8;
+    const uint32_t KP = (static_cast<uint32_t>(D) + 15) / 16 * 16;
+    const uint32_t NB = join_cols(K);
+    const uint32_t tiles_bytes = (kTile + NB) * KP * 2;
+    const uint32_t lists_bytes = kTile * list_stride(K) * 4;
     JoinSmem s{};
-    s.a = 0;
-    s.b = s.a + kTile * KP * 4;
-    s.norm_a = s.b + join_cols(K) * KP * 4;
+    s.rows_a = 0;
+    s.rows_b = s.rows_a + kTile * static_cast<uint32_t>(D) * 4;
+    s.tiles = (s.rows_b + NB * static_cast<uint32_t>(D) * 4 + 127) / 128 * 128;
+    s.tile_b = s.tiles + kTile * KP * 2;
+    s.norm_a = s.tiles + ((tiles_bytes > lists_bytes ? tiles_bytes : lists_bytes) + 15) / 16 * 16;
     s.norm_b = s.norm_a + kTile * 4;
-    s.bnd = s.norm_b + kTile * 4;
+    s.rt_a = s.norm_b + kTile * 4;
+    s.rt_b = s.rt_a + kTile * 4;
+    s.bnd = s.rt_b + kTile * 4;
     s.pid = s.bnd + kTile * 4;
     s.cid = s.pid + kTile * 4;
     s.fullrow = s.cid + kTile * 4;
     s.centre = s.fullrow + kTile * 4;
     s.x = s.centre + (static_cast<uint32_t>(D) + 3) / 4 * 16;
     // pair masks and member masks (u64 per thread each), prefix sums
-    // (kJoinThreads + 1), warp totals (8)
-    s.bytes = s.x + 2 * kJoinThreads * 8 + (kJoinThreads + 1) * 4 + 8 * 4;
+    // (kJoinThreads + 1), warp totals
+    s.bytes = s.x + 2 * kJoinThreads * 8 + (kJoinThreads + 1) * 4 + kJoinWarps * 4;
     return s;
-}
-
-// Row stride (in ids) of the staged sorted lists: k when k is a multiple of 4
-// (rows copied in 16-byte pieces), else odd when 128 such rows fit in the
-// tiles' space (searches by different rows spread over the banks).
-__host__ __device__ inline int list_stride(int D, uint32_t K) {
-    if ((K & 3u) == 0) return static_cast<int>(K);
-    const uint32_t KP = (D + 7) / 8 * 8;
-    const uint32_t space = (kTile + join_cols(K)) * KP * 4;
-    return static_cast<uint32_t>(kTile) * (K | 1u) * 4 <= space ? static_cast<int>(K | 1u) : static_cast<int>(K);
 }
 
 // Block-wide exclusive prefix sums of the set bits of every thread's pair
@@ -371,7 +378,7 @@ __device__ __forceinline__ void scan_masks_block(unsigned long long mask, uint32
     const int warp = threadIdx.x / kWarp;
     uint32_t before = 0, total = 0;
 #pragma unroll
-    for (int w = 0; w < kJoinThreads / kWarp; ++w) {
+    for (int w = 0; w < kJoinWarps; ++w) {
         const uint32_t s = wsum[w];
         before += w < warp ? s : 0u;
         total += s;
@@ -421,122 +428,99 @@ __device__ __forceinline__ void pair_next(PairCursor& c, const unsigned long lon
     ++c.lo;
 }
 
-// Tile row and column of bit `bit` of thread o's mask (thread o owns TMEM
-// lane (o / 32 % 4) * 32 + o % 32 and columns (o / 32 / 4) * 64 + bit).
+// Tile row and column of bit `bit` of thread o's mask: thread o reads TMEM
+// lane (o / 32 % 4) * 32 + o % 32 (its warp's lane quarter) and filters
+// columns (o / 32 / 4) * 32 + bit.
 __device__ __forceinline__ int pair_row(int o) { return ((o / kWarp) % 4) * kWarp + (o % kWarp); }
-__device__ __forceinline__ int pair_col(int o, int bit) { return ((o / kWarp) / 4) * 64 + bit; }
+__device__ __forceinline__ int pair_col(int o, int bit) { return ((o / kWarp) / 4) * kGroupCols + bit; }
 
-// rows[r] (r < count and ids[r] != kNone, else zeros) minus `centre`, into a
-// chunk-major tile of `rows` rows (a multiple of 8).  Every 16-byte chunk a
-// thread owns is first copied with cp.async (all of them in flight at once),
-// then centred in place by the same thread.  Lane l of a warp handles row
-// (8g + l % 8), chunk (4h + l / 8): every global sector read is used whole
-// and each quarter-warp's 16-byte shared accesses land on distinct banks.
+// Centred FP16 operand rows from FP32 rows in shared memory.  Two threads
+// per row (t = 2r + h; half h converts chunks [h*HALF, (h+1)*HALF)): row r
+// (r < count, else zeros) minus `centre`, rounded to FP16, into a
+// chunk-major tile of `R` rows (chunk c of row r at c*R*16 + r*16).  Writes
+// the row's squared norm (FP32, of the centred FP32 values; both halves
+// summed in a fixed order) and its absolute error term 2^-19 |x'| (+inf when
+// a value does not fit FP16's range, so that the filter keeps every pair of
+// the row).  All 32 lanes of a warp call it; t below 2R do work.
 template <int D>
-__device__ __forceinline__ void stage_centred(float* __restrict__ tile, uint32_t rows, const uint32_t* __restrict__ ids,
-                                              uint32_t count, const float* __restrict__ pts, int ld,
-                                              const float* __restrict__ centre) {
+__device__ __forceinline__ void convert_rows(const float* __restrict__ rows, uint32_t count, uint32_t R,
+                                             unsigned char* __restrict__ tile, const float* __restrict__ centre,
+                                             float* __restrict__ norm, float* __restrict__ rt, int t) {
     constexpr int CH = JoinLayout<D>::CH;
-    constexpr int CG = (CH + 3) / 4;  // chunk groups
-    constexpr int WARPS = kJoinThreads / kWarp;
-    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
-    const int rl = lane & 7, cl = lane >> 3;
-    const int groups = static_cast<int>(rows / 8);
-    const int tasks = groups * CG;
-    unsigned char* base = reinterpret_cast<unsigned char*>(tile);
-    // Task w = (chunk group w / groups, row group w % groups); this warp's
-    // tasks are warp, warp + WARPS, ...: the pair is advanced, not divided.
-    int g = warp, cg = 0;
-    while (g >= groups) {
-        g -= groups;
-        ++cg;
-    }
-    const int g0 = g, cg0 = cg;
+    constexpr int HALF = (CH + 1) / 2;
+    const uint32_t r = static_cast<uint32_t>(t) >> 1;
+    const int h = t & 1;
+    float s = 0.0f, mx = 0.0f;
+    if (r < R) {
+        const bool live = r < count;
 #pragma unroll 1
-    for (int w = warp; w < tasks; w += WARPS) {
-        const int r = g * 8 + rl, ch = cg * 4 + cl;
-        if (ch < CH) {
-            const bool valid = static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone;
-            const float* src = valid ? pts + static_cast<size_t>(ids[r]) * ld + 4 * ch : pts;
-            tc::cp_async16(base + tc::chunk_offset(r, 4 * ch, rows), src, valid);
-        }
-        g += WARPS;
-        while (g >= groups) {
-            g -= groups;
-            ++cg;
+        for (int i = 0; i < HALF; ++i) {
+            const int c = h * HALF + i;
+            if (c >= CH) break;
+            float v[8];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int k = 8 * c + 4 * q;
+                float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (live && k < D) {
+                    const float4 a = *reinterpret_cast<const float4*>(rows + static_cast<size_t>(r) * D + k);
+                    const float4 m = *reinterpret_cast<const float4*>(centre + k);
+                    x = make_float4(__fsub_rn(a.x, m.x), __fsub_rn(a.y, m.y), __fsub_rn(a.z, m.z), __fsub_rn(a.w, m.w));
+                }
+                v[4 * q + 0] = x.x;
+                v[4 * q + 1] = x.y;
+                v[4 * q + 2] = x.z;
+                v[4 * q + 3] = x.w;
+            }
+            uint4 packed;
+            uint32_t* pk = reinterpret_cast<uint32_t*>(&packed);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const __half2 hv = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
+                pk[e] = *reinterpret_cast<const uint32_t*>(&hv);
+            }
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                s = fmaf(v[e], v[e], s);
+                mx = fmaxf(mx, fabsf(v[e]));
+            }
+            *reinterpret_cast<uint4*>(tile + static_cast<size_t>(c) * R * 16 + static_cast<size_t>(r) * 16) = packed;
         }
     }
-    tc::cp_async_wait_all();
-    g = g0;
-    cg = cg0;
-#pragma unroll 1
-    for (int w = warp; w < tasks; w += WARPS) {
-        const int r = g * 8 + rl, ch = cg * 4 + cl;
-        if (ch < CH && static_cast<uint32_t>(r) < count && 4 * ch < D && ids[r] != kNone) {
-            float4* at = reinterpret_cast<float4*>(base + tc::chunk_offset(r, 4 * ch, rows));
-            const float4 x = *at;
-            const float4 m = reinterpret_cast<const float4*>(centre)[ch];
-            *at = make_float4(__fsub_rn(x.x, m.x), __fsub_rn(x.y, m.y), __fsub_rn(x.z, m.z), __fsub_rn(x.w, m.w));
-        }
-        g += WARPS;
-        while (g >= groups) {
-            g -= groups;
-            ++cg;
-        }
+    const float so = __shfl_xor_sync(kFull, s, 1);
+    const float mo = __shfl_xor_sync(kFull, mx, 1);
+    if (r < R && h == 0) {
+        const float nrm = s + so;
+        norm[r] = nrm;
+        rt[r] = fmaxf(mx, mo) >= 32768.0f ? __int_as_float(0x7f800000) : 1.9073486328125e-06f * sqrtf(nrm);
     }
 }
 
-// Squared norm of row r of a chunk-major tile (any order: only feeds the bound).
-template <int D>
-__device__ __forceinline__ float tile_norm(const float* __restrict__ tile, int r, uint32_t rows) {
-    constexpr int CH = JoinLayout<D>::CH;
-    float s = 0.f;
-#pragma unroll 4
-    for (int ch = 0; ch < CH; ++ch) {
-        const float4 v = *reinterpret_cast<const float4*>(reinterpret_cast<const unsigned char*>(tile) +
-                                                          tc::chunk_offset(r, 4 * ch, rows));
-        s = fmaf(v.x, v.x, fmaf(v.y, v.y, fmaf(v.z, v.z, fmaf(v.w, v.w, s))));
-    }
-    return s;
-}
-
-// Copies rows ids[r] (r < count, ids[r] != kNone) into a row-major tile of D
-// floats per row with cp.async (all of a thread's copies in flight at once);
-// the caller waits (cp_async_wait_all, then a barrier).
-template <int D>
-__device__ __forceinline__ void stage_rows(float* __restrict__ dst, const uint32_t* __restrict__ ids, uint32_t count,
-                                           const float* __restrict__ pts, int ld) {
-    constexpr int Q = D / 4;
-    const uint32_t total = count * Q;
-    uint32_t r = threadIdx.x / Q, q = threadIdx.x % Q;
-    constexpr uint32_t dr = kJoinThreads / Q, dq = kJoinThreads % Q;
-#pragma unroll 1
-    for (uint32_t f = threadIdx.x; f < total; f += kJoinThreads) {
-        const uint32_t id = ids[r];
-        if (id != kNone) tc::cp_async16(dst + static_cast<size_t>(f) * 4, pts + static_cast<size_t>(id) * ld + 4 * q, true);
-        r += dr;
-        q += dq;
-        if (q >= static_cast<uint32_t>(Q)) {
-            q -= Q;
-            ++r;
-        }
-    }
-}
-
-// The local join of one neighbour-of-neighbour pass.  For every point q: the
-// rows R(q) (points whose snapshot list holds q), in chunks of 128, against
-// the columns S(q) (q's snapshot list, distinct ids).  A tcgen05 TF32 tile of
-// centred dot products rejects the pairs that provably cannot beat bound(p);
-// members of S(p) are dropped (binary searches, four in lockstep, in S(p)
-// staged in shared memory); the remaining pairs get the exact FP32 distance,
-// spread evenly over the CTA's threads.  Every point's survivors (distance < bound(p)) are counted exactly
-// into surv_count.  A point's first `slots` survivors go to
-// surv[p * slots + cursor]; the rest to this CTA's pool region
-// pool[blockIdx.x * pool_cap ...] as (p, candidate, distance bits, 0).  When
+// The local join of one neighbour-of-neighbour pass.  For every point q (taken
+// in `order`, the last repetition's leaf order, through the work counter):
+// the rows R(q) (points whose snapshot list holds q), in chunks of 128,
+// against the columns S(q) (q's snapshot list, distinct ids).
+//
+// Per chunk: one warp issues a bulk copy per row (R(q) rows, and S(q) rows
+// when q is new) into shared memory; the CTA builds the centred FP16 tiles
+// from them; one thread issues the tcgen05.mma (kind::f16, FP32 accumulate)
+// into TMEM; while the lists S(p) of the chunk's rows are bulk-copied into the
+// tile space, every thread filters 32 accumulator columns of its TMEM lane:
+// a pair is kept unless approx - margin >= bound(p), with
+//   margin = 2^-8 (|x'|^2 + |y'|^2) + 2^-16 |approx| + 2^-19 (|x'| + |y'|)
+// covering FP16 rounding of both operands (2^-11 relative, 2^-25 absolute in
+// the subnormal range), FP32 accumulation, the centring rounding and the
+// reference's own summation order.  Members of S(p) are then dropped (branch-
+// free binary searches, four in lockstep), and the remaining pairs get the
+// exact FP32 distance in the reference's order from the staged rows, spread
+// evenly over the CTA's threads.  Every point's survivors (distance <
+// bound(p)) are counted exactly into surv_count; a point's first `slots` go to
+// surv[p * slots + cursor], the rest to this CTA's pool region
+// pool[blockIdx.x * pool_cap ...] as (p, candidate, distance bits, 0); when
 // the region is full the record is dropped and lost[p] set; the CTA's final
 // pool fill is written to pool_fill[blockIdx.x].
 template <int D>
-__global__ void __launch_bounds__(kJoinThreads, 2)
+__global__ void __launch_bounds__(kJoinThreads, 1)
     k_join(const uint32_t* __restrict__ snap, const unsigned long long* __restrict__ rev_off,
            const uint32_t* __restrict__ rev, const float* __restrict__ pts, int ld, const float* __restrict__ bound,
            const uint32_t* __restrict__ set_size, int K, uint32_t n, uint32_t slots,
@@ -548,10 +532,15 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     extern __shared__ __align__(1024) unsigned char smem[];
     const JoinSmem S = join_smem(D, static_cast<uint32_t>(K));
     const uint32_t NB = join_cols(static_cast<uint32_t>(K));
-    float* A = reinterpret_cast<float*>(smem + S.a);
-    float* B = reinterpret_cast<float*>(smem + S.b);
+    float* rows_a = reinterpret_cast<float*>(smem + S.rows_a);
+    float* rows_b = reinterpret_cast<float*>(smem + S.rows_b);
+    unsigned char* tile_a = smem + S.tiles;
+    unsigned char* tile_b = smem + S.tile_b;
+    uint32_t* lists = reinterpret_cast<uint32_t*>(smem + S.tiles);
     float* normA = reinterpret_cast<float*>(smem + S.norm_a);
     float* normB = reinterpret_cast<float*>(smem + S.norm_b);
+    float* rtA = reinterpret_cast<float*>(smem + S.rt_a);
+    float* rtB = reinterpret_cast<float*>(smem + S.rt_b);
     float* bnd = reinterpret_cast<float*>(smem + S.bnd);
     uint32_t* pid = reinterpret_cast<uint32_t*>(smem + S.pid);
     uint32_t* cid = reinterpret_cast<uint32_t*>(smem + S.cid);
@@ -560,36 +549,49 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     unsigned long long* todo_s = reinterpret_cast<unsigned long long*>(smem + S.x);   // [kJoinThreads]
     unsigned long long* mem_s = todo_s + kJoinThreads;                                // [kJoinThreads]
     uint32_t* pref = reinterpret_cast<uint32_t*>(smem + S.x + 2 * kJoinThreads * 8);  // [kJoinThreads + 1]
-    uint32_t* wsum = pref + kJoinThreads + 1;                                          // [8]
-    __shared__ uint64_t mbar;
+    uint32_t* wsum = pref + kJoinThreads + 1;                                          // [kJoinWarps]
+    __shared__ uint64_t rows_bar, list_bar, mma_bar;
     __shared__ uint32_t tmem_slot;
     __shared__ uint32_t ncols_s;
     __shared__ uint32_t pool_cursor;
+    __shared__ uint32_t work_s[2];
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
     if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
     if (tid == 0) {
         pool_cursor = 0;
-        tc::mbar_init(&mbar, 1);
+        tc::mbar_init(&rows_bar, 1);
+        tc::mbar_init(&list_bar, 1);
+        tc::mbar_init(&mma_bar, 1);
         tc::fence_barrier_init();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    const uint32_t idesc = tc::idesc_tf32(kTile, NB);
-    uint32_t phase = 0;
+    const uint32_t idesc = tc::idesc_f16(kTile, NB);
+    const bool bulk_lists = (K & 3) == 0;
+    const int KS = static_cast<int>(list_stride(static_cast<uint32_t>(K)));
+    constexpr uint32_t kRowBytes = D * sizeof(float);
+    uint32_t ph_rows = 0, ph_list = 0, ph_mma = 0;
     bool healthy = true;
     unsigned long long n_pairs = 0, n_pass = 0, n_member = 0, n_exact = 0, n_emit = 0;
-    const int quarter = warp % 4, half = warp / 4;
-    const int row = quarter * kWarp + lane;  // TMEM lane / tile row of this thread
+    const int quarter = warp % 4, group = warp / 4;
+    const int row = quarter * kWarp + lane;  // TMEM lane / tile row this thread filters
     const unsigned lt = (1u << lane) - 1u;
-    const int KS = list_stride(D, static_cast<uint32_t>(K));
     int search_top = 1;  // largest power of two <= K (branch-free lower bound)
     while (search_top * 2 <= K) search_top *= 2;
-    // Work: positions of `order` (the last repetition's leaf order, so that
-    // the CTAs running at the same time take neighbouring points, whose rows
-    // and lists overlap and stay in L2), handed out one at a time.
-    __shared__ uint32_t work_s[2];
+    // Waits on this CTA's own copies and MMAs; a wait that gives up marks the
+    // launch failed, and waits once more with the full limit (the copies in
+    // flight land before the CTA exits).
+    auto wait_or_fail = [&](uint64_t* bar, uint32_t parity) -> bool {
+        const bool done = tc::mbar_wait_limited(bar, parity);
+        if (__syncthreads_or(!done)) {
+            if (tid == 0) atomicExch(error_flag, 1u);
+            tc::mbar_wait(bar, parity);
+            return false;
+        }
+        return true;
+    };
     for (uint32_t it = 0; healthy; ++it) {
         if (tid == 0) work_s[it & 1u] = atomicAdd(work, 1u);
         __syncthreads();
@@ -625,133 +627,118 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
         for (int j = tid; j < D; j += kJoinThreads) centre[j] = pts[static_cast<size_t>(q) * ld + j];
         __syncthreads();
         const uint32_t nc = ncols_s;
-        stage_centred<D>(B, NB, cid, nc, pts, ld, centre);
-        __syncthreads();
-        if (static_cast<uint32_t>(tid) < NB) normB[tid] = tile_norm<D>(B, tid, NB);
         for (unsigned long long cb = rb; cb < re && healthy; cb += kTile) {
             const uint32_t m = static_cast<uint32_t>(min(static_cast<unsigned long long>(kTile), re - cb));
-            bool any = false;
+            const bool with_b = cb == rb;
             if (tid < kTile) {
                 const uint32_t p = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
                 pid[tid] = p;
                 bnd[tid] = p != kNone ? bound[p] : 0.0f;
                 fullrow[tid] = p != kNone && set_size[p] == static_cast<uint32_t>(K) ? 1u : 0u;
-                any = p != kNone;
             }
-            if (!__syncthreads_or(any)) continue;
-            stage_centred<D>(A, kTile, pid, m, pts, ld, centre);
             __syncthreads();
-            if (tid < kTile) normA[tid] = tile_norm<D>(A, tid, kTile);
+            // The chunk's rows (and S(q)'s for a new q): one bulk copy per row.
+            if (warp == 0) {
+                if (lane == 0) tc::mbar_arrive_expect_tx(&rows_bar, (m + (with_b ? nc : 0u)) * kRowBytes);
+                __syncwarp();
+                for (uint32_t r = lane; r < m; r += kWarp)
+                    tc::bulk_g2s(rows_a + static_cast<size_t>(r) * D, pts + static_cast<size_t>(pid[r]) * ld, kRowBytes,
+                                 &rows_bar);
+                if (with_b)
+                    for (uint32_t j = lane; j < nc; j += kWarp)
+                        tc::bulk_g2s(rows_b + static_cast<size_t>(j) * D, pts + static_cast<size_t>(cid[j]) * ld,
+                                     kRowBytes, &rows_bar);
+            }
+            if (!wait_or_fail(&rows_bar, ph_rows)) {
+                healthy = false;
+                break;
+            }
+            ph_rows ^= 1u;
+            // Centred FP16 operand tiles, norms and error terms.
+            if (tid < 2 * kTile)
+                convert_rows<D>(rows_a, m, kTile, tile_a, centre, normA, rtA, tid);
+            else
+                convert_rows<D>(rows_b, nc, NB, tile_b, centre, normB, rtB, tid - 2 * kTile);
             tc::fence_proxy_async();
             tc::fence_before_sync();
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after_sync();
-                tc::issue_tile_tf32(tmem, tc::smem_u32(A), tc::smem_u32(B), kTile, NB, L::KP, idesc);
-                tc::mma_commit(&mbar);
+                tc::issue_tile_16bit(tmem, tc::smem_u32(tile_a), tc::smem_u32(tile_b), kTile, NB, L::KP, idesc);
+                tc::mma_commit(&mma_bar);
             }
-            const bool done = tc::mbar_wait(&mbar, phase);
-            phase ^= 1u;
-            if (__syncthreads_or(!done)) {
-                if (tid == 0) atomicExch(error_flag, 1u);
+            if (!wait_or_fail(&mma_bar, ph_mma)) {
                 healthy = false;
                 break;
             }
+            ph_mma ^= 1u;
             tc::fence_after_sync();
-            // p's list S(p), sorted, staged into the space A' and B' occupied
-            // (row stride KS).
-            {
-                uint32_t* dst = reinterpret_cast<uint32_t*>(A);
-                const uint32_t total = m * static_cast<uint32_t>(K);
-                if ((K & 3) == 0) {
-                    // 16-byte cp.async pieces (row stride KS = K), all in flight.
-                    const uint32_t KV = static_cast<uint32_t>(K) / 4, tv = total / 4;
-                    uint32_t r = static_cast<uint32_t>(tid) / KV, a = static_cast<uint32_t>(tid) % KV;
-                    const uint32_t dr = kJoinThreads / KV, da = kJoinThreads % KV;
-#pragma unroll 1
-                    for (uint32_t f = tid; f < tv; f += kJoinThreads) {
-                        const uint32_t pr = pid[r];
-                        if (pr != kNone)
-                            tc::cp_async16(dst + static_cast<size_t>(f) * 4,
-                                           snap + static_cast<size_t>(pr) * K + 4 * a, true);
-                        r += dr;
-                        a += da;
-                        if (a >= KV) {
-                            a -= KV;
-                            ++r;
-                        }
-                    }
-                    tc::cp_async_wait_all();
-                } else {
-#pragma unroll 1
-                    for (uint32_t f0 = tid; f0 < total; f0 += 4 * kJoinThreads) {
-                        uint32_t v[4];
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const uint32_t f = f0 + u * kJoinThreads;
-                            v[u] = kNone;
-                            if (f < total) {
-                                const uint32_t r = f / K, a = f - r * K;
-                                const uint32_t pr = pid[r];
-                                if (pr != kNone) v[u] = __ldg(snap + static_cast<size_t>(pr) * K + a);
-                            }
-                        }
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const uint32_t f = f0 + u * kJoinThreads;
-                            if (f < total) {
-                                const uint32_t r = f / K, a = f - r * K;
-                                dst[r * KS + a] = v[u];
-                            }
-                        }
-                    }
-                }
-                __syncthreads();
+            // The tiles are consumed: the chunk's lists S(p) go into their space
+            // (one bulk copy per list) while the filter runs.
+            if (bulk_lists && warp == 0) {
+                if (lane == 0) tc::mbar_arrive_expect_tx(&list_bar, m * static_cast<uint32_t>(K) * 4u);
+                __syncwarp();
+                for (uint32_t r = lane; r < m; r += kWarp)
+                    tc::bulk_g2s(lists + static_cast<size_t>(r) * KS, snap + static_cast<size_t>(pid[r]) * K,
+                                 static_cast<uint32_t>(K) * 4u, &list_bar);
             }
-            // Filter: bit (cc*16 + u) of `todo` marks column half*64 + cc*16 + u
-            // as a pair that may beat bound(p) and is not a member of S(p).
+            // Filter: bit u of `todo` marks column group*32 + u as a pair that
+            // may beat bound(p).
             const uint32_t p = row < static_cast<int>(m) ? pid[row] : kNone;
             const float bp = row < static_cast<int>(m) ? bnd[row] : 0.0f;
             unsigned long long todo = 0;
             {
-                const float na = normA[row];
-#pragma unroll 1
-                for (int cc = 0; cc < 4; ++cc) {
-                    const int j0 = half * 64 + cc * 16;
-                    if (j0 >= static_cast<int>(nc)) break;  // warp-uniform
-                    float g[16];
-                    tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
-                    tc::tmem_wait_ld();
-                    // |approx - exact| <= 2^-7 (|x'|^2 + |y'|^2) + 2^-16 |approx| covers the TF32
-                    // operands, FP32 accumulation, centring and the reference's summation order.
+                const float na = normA[row], ra = rtA[row];
+                const int j0 = group * kGroupCols;
+                if (j0 < static_cast<int>(nc)) {  // warp-uniform
                     uint32_t pass = 0;
-                    float nbv[16];
 #pragma unroll
-                    for (int u4 = 0; u4 < 4; ++u4) {
-                        const float4 t4 = reinterpret_cast<const float4*>(normB + j0)[u4];
-                        nbv[4 * u4 + 0] = t4.x;
-                        nbv[4 * u4 + 1] = t4.y;
-                        nbv[4 * u4 + 2] = t4.z;
-                        nbv[4 * u4 + 3] = t4.w;
-                    }
+                    for (int hh = 0; hh < 2; ++hh) {
+                        const int jb = j0 + 16 * hh;
+                        if (jb >= static_cast<int>(nc)) break;  // warp-uniform
+                        float g[16];
+                        tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + jb, g);
+                        tc::tmem_wait_ld();
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) {
-                        const float nb = nbv[u];
-                        const float approx = na + nb - 2.0f * g[u];
-                        const float margin = 0.0078125f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + 1e-30f;
-                        if (approx - margin < bp) pass |= 1u << u;
+                        for (int u = 0; u < 16; ++u) {
+                            const float nb = normB[jb + u];
+                            const float approx = na + nb - 2.0f * g[u];
+                            const float margin = 0.00390625f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + ra +
+                                                 rtB[jb + u];
+                            // NaN-safe: a pair is dropped only when the bound provably holds.
+                            if (!(approx - margin >= bp)) pass |= 1u << (16 * hh + u);
+                        }
                     }
-                    const int valid_cols = max(0, min(16, static_cast<int>(nc) - j0));
-                    pass &= valid_cols == 16 ? 0xFFFFu : ((1u << valid_cols) - 1u);
+                    const int valid_cols = max(0, min(kGroupCols, static_cast<int>(nc) - j0));
+                    pass &= valid_cols == kGroupCols ? 0xFFFFFFFFu : ((1u << valid_cols) - 1u);
                     if (p == kNone) pass = 0;
                     if (p != kNone) {
                         n_pairs += valid_cols;
                         n_pass += __popc(pass);
                     }
-                    todo |= static_cast<unsigned long long>(pass) << (cc * 16);
+                    todo = pass;
                 }
             }
-            // Filter-passing pairs of the block, then the members of S(p)
+            if (!bulk_lists) {
+                // Lists whose rows are not 16-byte multiples: plain loads.
+                __syncthreads();
+                const uint32_t total = m * static_cast<uint32_t>(K);
+#pragma unroll 1
+                for (uint32_t f0 = tid; f0 < total; f0 += 4 * kJoinThreads) {
+                    uint32_t v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t f = f0 + u * kJoinThreads;
+                        v[u] = f < total ? __ldg(snap + static_cast<size_t>(pid[f / K]) * K + f % K) : kNone;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t f = f0 + u * kJoinThreads;
+                        if (f < total) lists[(f / K) * KS + f % K] = v[u];
+                    }
+                }
+            }
+            // Filter-passing pairs of the chunk, then the members of S(p)
             // among them (rejected by the set update: dropped), an even share
             // of the pairs per thread, lower bounds of four at a time
             // (branch-free, in lockstep).  A set that is not full lists its
@@ -760,12 +747,15 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
             todo_s[tid] = todo;
             mem_s[tid] = 0ull;
             uint32_t incl = scan_masks_warp(todo, wsum);
-            tc::fence_before_sync();
             __syncthreads();
             scan_masks_block(todo, incl, wsum, pref);
+            if (bulk_lists && !wait_or_fail(&list_bar, ph_list)) {
+                healthy = false;
+                break;
+            }
+            if (bulk_lists) ph_list ^= 1u;
             __syncthreads();
             {
-                const uint32_t* lists = reinterpret_cast<const uint32_t*>(A);
                 PairCursor cur = pair_share(pref, todo_s);
 #pragma unroll 1
                 while (cur.lo < cur.hi) {
@@ -803,20 +793,14 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                 }
             }
             __syncthreads();
-            // The remaining pairs and their prefix sums, then the original
-            // FP32 rows in the tiles' space (the lists are consumed).
+            // The remaining pairs, an even share per thread: exact distances
+            // from the staged original rows.
             todo &= ~mem_s[tid];
             incl = scan_masks_warp(todo, wsum);
             todo_s[tid] = todo;
-            float* Aorig = A;
-            float* Bo = B;
-            stage_rows<D>(Aorig, pid, m, pts, ld);
-            stage_rows<D>(Bo, cid, nc, pts, ld);
-            tc::cp_async_wait_all();
             __syncthreads();
             scan_masks_block(todo, incl, wsum, pref);
             __syncthreads();
-            // Exact distances over an even share of the remaining pairs.
             {
                 PairCursor cur = pair_share(pref, todo_s);
 #pragma unroll 1
@@ -829,8 +813,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                     const uint32_t c = cid[j];
                     if (c == pp) continue;
                     ++n_exact;
-                    const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(Bo + j * D),
-                                                                reinterpret_cast<const float4*>(Aorig + prow * D));
+                    const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(rows_b + j * D),
+                                                                reinterpret_cast<const float4*>(rows_a + prow * D));
                     if (d < bnd[prow]) {
                         ++n_emit;
                         const uint32_t s = atomicAdd(&surv_count[pp], 1u);
@@ -848,12 +832,11 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
                     }
                 }
             }
+            // Every thread is done with the rows, lists and TMEM before the
+            // next chunk's copies and MMA.
+            tc::fence_before_sync();
             __syncthreads();
-            // The next chunk restages B' (its space now holds original rows).
-            if (cb + kTile < re) {
-                stage_centred<D>(B, NB, cid, nc, pts, ld, centre);
-                __syncthreads();
-            }
+            tc::fence_after_sync();
         }
     }
     atomicAdd(&counters[0], n_pairs);
@@ -861,6 +844,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2)
     atomicAdd(&counters[2], n_member);
     atomicAdd(&counters[3], n_exact);
     atomicAdd(&counters[4], n_emit);
+    tc::fence_before_sync();
     __syncthreads();
     if (tid == 0) pool_fill[blockIdx.x] = min(pool_cursor, pool_cap);
     if (warp == 0) {
@@ -957,7 +941,8 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
     }
 }
 
-// One 128 x 128 TF32 tile of a(m x D) . b(n x D)^T (rows past m / n are zero);
+// One 128 x 128 tile of the join's filter: a(m x D) . b(n x D)^T with both
+// operands rounded to FP16 and FP32 accumulation (rows past m / n are zero);
 // the diagnostic behind knng_debug_tile_gram.
 template <int D>
 __global__ void __launch_bounds__(kJoinThreads, 1)
@@ -965,14 +950,21 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                 float* __restrict__ out, uint32_t* __restrict__ error_flag) {
     using L = JoinLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
-    float* A = reinterpret_cast<float*>(smem);
-    float* B = reinterpret_cast<float*>(smem + L::tile_bytes);
-    uint32_t* ids = reinterpret_cast<uint32_t*>(smem + 2 * L::tile_bytes);
-    float* zero = reinterpret_cast<float*>(ids + kTile);
+    const JoinSmem S = join_smem(D, kTile);
+    float* rows_a = reinterpret_cast<float*>(smem + S.rows_a);
+    float* rows_b = reinterpret_cast<float*>(smem + S.rows_b);
+    unsigned char* tile_a = smem + S.tiles;
+    unsigned char* tile_b = smem + S.tile_b;
+    float* norm_a = reinterpret_cast<float*>(smem + S.norm_a);
+    float* norm_b = reinterpret_cast<float*>(smem + S.norm_b);
+    float* rt_a = reinterpret_cast<float*>(smem + S.rt_a);
+    float* rt_b = reinterpret_cast<float*>(smem + S.rt_b);
+    float* zero = reinterpret_cast<float*>(smem + S.centre);
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
-    if (tid < kTile) ids[tid] = tid;
+    for (uint32_t f = tid; f < m * D; f += kJoinThreads) rows_a[f] = a[f];
+    for (uint32_t f = tid; f < n * D; f += kJoinThreads) rows_b[f] = b[f];
     for (int j = tid; j < D; j += kJoinThreads) zero[j] = 0.0f;
     if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
     if (tid == 0) {
@@ -983,24 +975,28 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    stage_centred<D>(A, kTile, ids, m, a, D, zero);
-    stage_centred<D>(B, kTile, ids, n, b, D, zero);
+    if (tid < 2 * kTile)
+        convert_rows<D>(rows_a, m, kTile, tile_a, zero, norm_a, rt_a, tid);
+    else
+        convert_rows<D>(rows_b, n, kTile, tile_b, zero, norm_b, rt_b, tid - 2 * kTile);
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
     if (tid == 0) {
         tc::fence_after_sync();
-        tc::issue_tile_tf32(tmem, tc::smem_u32(A), tc::smem_u32(B), kTile, kTile, L::KP, tc::idesc_tf32(kTile, kTile));
+        tc::issue_tile_16bit(tmem, tc::smem_u32(tile_a), tc::smem_u32(tile_b), kTile, kTile, L::KP,
+                             tc::idesc_f16(kTile, kTile));
         tc::mma_commit(&mbar);
     }
     const bool done = tc::mbar_wait(&mbar, 0);
     if (__syncthreads_or(!done)) {
         if (tid == 0) atomicExch(error_flag, 1u);
+        tc::mbar_wait(&mbar, 0);
     } else {
         tc::fence_after_sync();
-        const int quarter = warp % 4, half = warp / 4, row = quarter * kWarp + lane;
-        for (int cc = 0; cc < 4; ++cc) {
-            const int j0 = half * 64 + cc * 16;
+        const int quarter = warp % 4, group = warp / 4, row = quarter * kWarp + lane;
+        for (int hh = 0; hh < 2; ++hh) {
+            const int j0 = group * kGroupCols + 16 * hh;
             float g[16];
             tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
             tc::tmem_wait_ld();
@@ -1077,11 +1073,13 @@ __global__ void __launch_bounds__(256) k_pool_scatter(const uint4* __restrict__ 
 
 }  // namespace
 
+void set_refine_wait_limit(uint32_t polls) { KNNG_CUDA(cudaMemcpyToSymbol(tc::g_wait_limit, &polls, sizeof(polls))); }
+
 void run_tile_gram(Context& c, uint32_t d, const float* d_a, uint32_t m, const float* d_b, uint32_t n, float* d_out) {
     auto* err = static_cast<uint32_t*>(scratch(c, "gram_error", sizeof(uint32_t)));
     KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
     KNNG_DISPATCH_D(d, {
-        const size_t smem = 2 * JoinLayout<D>::tile_bytes + kTile * 4 + D * 4;
+        const size_t smem = join_smem(D, kTile).bytes;
         auto kern = k_tile_gram<D>;
         allow_max_smem(c, kern);
         kern<<<1, kJoinThreads, smem, c.stream>>>(d_a, m, d_b, n, d_out, err);
@@ -1090,7 +1088,7 @@ void run_tile_gram(Context& c, uint32_t d, const float* d_a, uint32_t m, const f
     KNNG_CUDA(cudaGetLastError());
     uint32_t h = 0;
     download(c, &h, err, 1);
-    if (h) fail(KNNG_ERR_CUDA, "tensor-core tile: the MMA completion wait timed out");
+    if (h) fail(KNNG_ERR_CUDA, "tensor-core tile: the MMA completion wait gave up");
 }
 
 uint64_t run_refine_pointwise(Context& c, const uint32_t* snap, const uint32_t* d_list, uint32_t count) {
@@ -1149,8 +1147,7 @@ uint64_t run_refine(Context& c) {
     c.launches += 2;
     KNNG_CUDA(cudaGetLastError());
 
-    // Join grid: as many CTAs as fit on the SMs at once (two per SM at
-    // d = 100, k = 100); each owns one pool region.
+    // Join grid: one persistent CTA per SM; each owns one pool region.
     const uint32_t join_bytes = join_smem(static_cast<int>(c.d), static_cast<uint32_t>(K)).bytes;
     // CTAs per SM from the SM's shared memory and registers (the kernel's
     // launch bounds ask for two).
@@ -1170,7 +1167,7 @@ uint64_t run_refine(Context& c) {
     const size_t per_cta_smem = join_bytes + fa.sharedSizeBytes + static_cast<size_t>(smem_reserved);
     const int by_smem = static_cast<int>(static_cast<size_t>(smem_sm) / per_cta_smem);
     const int by_regs = fa.numRegs > 0 ? regs_sm / (fa.numRegs * kJoinThreads) : 2;
-    const int per_sm = std::min({by_smem, by_regs, 2});
+    const int per_sm = std::min({by_smem, by_regs, 1});
     if (per_sm < 1) fail(KNNG_ERR_UNSUPPORTED, "the join kernel does not fit on an SM");
     const uint32_t kJoinBlocks = static_cast<uint32_t>(sms) * static_cast<uint32_t>(per_sm);
     // Survivor storage: `slots` per point, then per-CTA pool regions for the
@@ -1255,7 +1252,7 @@ uint64_t run_refine(Context& c) {
     download(c, &herr, err, 1);
     if (herr) {
         for (auto& e : ev) cudaEventDestroy(e);
-        fail(KNNG_ERR_CUDA, "tensor-core join: an MMA completion wait timed out");
+        fail(KNNG_ERR_CUDA, "tensor-core join: a copy or MMA completion wait gave up");
     }
     const uint32_t max_count = hc32[2], lost_points = hc32[3];
     auto* ovf = static_cast<unsigned long long*>(

@@ -530,6 +530,8 @@ __global__ void k_copy_back(const Item* __restrict__ items, const uint32_t* __re
 
 }  // namespace
 
+void set_split_wait_limit(uint32_t polls) { KNNG_CUDA(cudaMemcpyToSymbol(tc::g_wait_limit, &polls, sizeof(polls))); }
+
 void launch_iota(Context& c) {
     if (c.n == 0) return;
     k_iota<<<std::min<uint32_t>((c.n + 255) / 256, 148 * 16), 256, 0, c.stream>>>(c.indices, c.n);

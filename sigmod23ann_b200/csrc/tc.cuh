@@ -240,11 +240,22 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t desc_a, uint6
         : "memory");
 }
 
-// Issues the K/16 MMAs of one 128 x N BF16 tile (call from a single thread).
-// The operand tiles use the same chunk-major layout as the TF32 ones, a
-// 16-byte chunk holding 8 BF16 values; one MMA consumes K = 16 (two chunks).
-__device__ __forceinline__ void issue_tile_bf16(uint32_t tmem_d, uint32_t a_base, uint32_t b_base, uint32_t a_rows,
-                                                uint32_t b_rows, uint32_t kpad, uint32_t idesc) {
+// Instruction descriptor: kind::f16 with FP16 A and B, F32 accumulate, both
+// K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_f16(uint32_t M, uint32_t N) {
+    return (1u << 4)                // D format: F32
+           | (0u << 7)              // A format: F16
+           | (0u << 10)             // B format: F16
+           | ((N >> 3) << 17)       // N / 8
+           | ((M >> 4) << 24);      // M / 16
+}
+
+// Issues the K/16 MMAs of one 128 x N 16-bit tile (call from a single thread).
+// The operand tiles (FP16 or BF16, as idesc says) use the same chunk-major
+// layout as the TF32 ones, a 16-byte chunk holding 8 values; one MMA consumes
+// K = 16 (two chunks).
+__device__ __forceinline__ void issue_tile_16bit(uint32_t tmem_d, uint32_t a_base, uint32_t b_base, uint32_t a_rows,
+                                                 uint32_t b_rows, uint32_t kpad, uint32_t idesc) {
     for (uint32_t s = 0; s < kpad / 16; ++s) {
         const uint64_t da = smem_desc(a_base + 2 * s * a_rows * 16, a_rows * 16, 128);
         const uint64_t db = smem_desc(b_base + 2 * s * b_rows * 16, b_rows * 16, 128);

@@ -22,8 +22,10 @@ def _recall(pts, ids, k, queries):
     return groundtruth.recall(ids.astype(np.int64), gt, queries)
 
 
-@pytest.mark.parametrize("max_leaf", [257, 513])
+@pytest.mark.parametrize("max_leaf", [257, 513, 1025])
 def test_bf16_rerank_recall_and_exact_distances(oracle_lib, max_leaf):
+    """Buckets of up to 256, 512 and 1024 points (the last one reads eight
+    128-column tiles per row block through the heap selection)."""
     pts = workloads.gaussian_mixture(n=20_000, d=100, clusters=64, sigma=0.15, seed=0)
     common = dict(reps=4, refine=1, max_leaf=max_leaf, max_leaf_odd=0, lloyd_iters=2, seed=11)
     with KnngContext(0) as ctx:
@@ -43,12 +45,13 @@ def test_bf16_rerank_recall_and_exact_distances(oracle_lib, max_leaf):
 
 
 def test_bf16_rerank_rejects_large_buckets():
+    """Buckets above 1024 points (max_leaf above 1025) are refused."""
     from sigmod23ann_b200 import KnngError
 
     pts = workloads.gaussian_mixture(n=2_000, d=100, clusters=4, seed=1)
     with KnngContext(0) as ctx:
         with pytest.raises(KnngError) as e:
-            ctx.build(pts, default_params(precision=PRECISION_BF16_RERANK, max_leaf=1025, max_leaf_odd=0))
+            ctx.build(pts, default_params(precision=PRECISION_BF16_RERANK, max_leaf=1026, max_leaf_odd=0))
     assert e.value.status == 6
 
 
