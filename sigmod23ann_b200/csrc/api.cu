@@ -609,7 +609,6 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     if (const char* r = std::getenv("KNNG_REFINE")) c->refine_mode = std::strcmp(r, "pointwise") == 0 ? 1 : 0;
     if (const char* r = std::getenv("KNNG_REFINE_SLOTS")) c->refine_slots = std::max(0, std::atoi(r));
     if (const char* r = std::getenv("KNNG_JOIN_ORDER")) c->join_order_ids = std::strcmp(r, "id") == 0;
-    if (const char* r = std::getenv("KNNG_LEAF_CTAS")) c->leaf_ctas_per_sm = std::atoi(r) == 1 ? 1 : 2;
     if (const char* r = std::getenv("KNNG_REFINE_POOL")) c->refine_pool = std::max<long long>(0, std::atoll(r));
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {

@@ -301,74 +301,6 @@ __device__ __forceinline__ uint32_t set_offer_batch(WarpSet& s, uint32_t cand, f
     return changed;
 }
 
-// The update of set_offer_batch for U independent sets at once (the four
-// points a warp owns in the bucket kernel), each offered 64 candidates in
-// column order: lane l holds column l in c[u][0] / d[u][0] and column 32 + l in
-// c[u][1] / d[u][1]; a column that is not an offer has distance +inf (never
-// below a bound, which is at most FLT_MAX).  Each step takes the next pending
-// offer of every set that has one, so the sets' dependency chains (shuffles,
-// membership vote, arg-max reductions, bound) interleave; every set sees
-// exactly the offers, in exactly the order, of set_offer_batch.
-template <int U>
-__device__ __forceinline__ void set_offer_multi(WarpSet (&s)[U], const uint32_t (&c)[U][2], const float (&d)[U][2],
-                                                int K, int lane) {
-    unsigned long long pend[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const unsigned lo = __ballot_sync(kFull, d[u][0] < s[u].bound);
-        const unsigned hi = __ballot_sync(kFull, d[u][1] < s[u].bound);
-        pend[u] = (static_cast<unsigned long long>(hi) << 32) | lo;
-    }
-    for (;;) {
-        unsigned long long any = 0;
-#pragma unroll
-        for (int u = 0; u < U; ++u) any |= pend[u];
-        if (any == 0) break;
-        bool acc[U], need[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const bool act = pend[u] != 0;
-            const int t = act ? __ffsll(static_cast<long long>(pend[u])) - 1 : 0;
-            pend[u] &= pend[u] - 1;
-            const bool high = t >= 32;
-            const float dj = __shfl_sync(kFull, high ? d[u][1] : d[u][0], t & 31);
-            const uint32_t cj = __shfl_sync(kFull, high ? c[u][1] : c[u][0], t & 31);
-            bool hit = false;
-#pragma unroll
-            for (int r = 0; r < kSlotsPerLane; ++r) {
-                const uint32_t slot = lane + r * kWarp;
-                hit |= (slot < s[u].size) && (s[u].id[r] == cj);
-            }
-            acc[u] = act && dj < s[u].bound && !__any_sync(kFull, hit);
-            const bool filling = s[u].size < static_cast<uint32_t>(K);
-            const uint32_t slot = acc[u] ? (filling ? s[u].size : s[u].maxslot) : kNone;
-            set_write_slot(s[u], slot, cj, dj, lane);
-            s[u].size += (acc[u] && filling) ? 1u : 0u;
-            need[u] = acc[u] && s[u].size == static_cast<uint32_t>(K);
-        }
-        bool all = true;
-#pragma unroll
-        for (int u = 0; u < U; ++u) all = all && need[u];
-        if (all) {
-#pragma unroll
-            for (int u = 0; u < U; ++u) warp_argmax(s[u], K, lane);
-        } else {
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (need[u]) warp_argmax(s[u], K, lane);
-        }
-        // The bounds only decrease: drop the offers they now exclude.
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (acc[u]) {
-                const unsigned lo = __ballot_sync(kFull, d[u][0] < s[u].bound);
-                const unsigned hi = __ballot_sync(kFull, d[u][1] < s[u].bound);
-                pend[u] &= (static_cast<unsigned long long>(hi) << 32) | lo;
-            }
-        }
-    }
-}
-
 // Ascending bitonic sort of n (power of two, n >= 2) 64-bit keys by one warp;
 // keys may live in shared or global memory.
 __device__ __forceinline__ void warp_bitonic_sort(unsigned long long* keys, uint32_t n, int lane) {

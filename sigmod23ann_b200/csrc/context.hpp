@@ -87,9 +87,6 @@ struct Context {
     // The join takes points in the leaf order of the last repetition; true
     // (environment KNNG_JOIN_ORDER=id at creation): in id order.
     bool join_order_ids = false;
-    // Bucket-kernel CTAs per SM the kernel is compiled for (register budget):
-    // 2 (64 registers a thread) or 1 (128); environment KNNG_LEAF_CTAS.
-    int leaf_ctas_per_sm = 2;
     int64_t refine_pool = -1;
     // Breakdown of the last refinement pass.
     struct RefineRecord {

@@ -9,7 +9,7 @@
 // walks the bucket in 64-point column blocks in ascending order, computes the
 // 64x64 distance block in the reference's FP32 order from dim-major shared
 // memory tiles, then each warp replays its points' 64 offers in column order
-// (set_offer_multi: the four points' updates interleaved step by step).  Distances are computed for the full b x b matrix (both
+// (set_offer_batch).  Distances are computed for the full b x b matrix (both
 // triangles); each (i, j) and (j, i) evaluation gives the same bits.
 #include <cuda_runtime.h>
 
@@ -93,8 +93,8 @@ __device__ __forceinline__ void distance_block(const float* __restrict__ I, cons
     for (int q = 0; q < kJPerThread; ++q) Dm[i * kDmStride + jg * kJPerThread + q] = tot[q];
 }
 
-template <int D, int MINB>
-__global__ void __launch_bounds__(kLeafThreads, MINB)
+template <int D>
+__global__ void __launch_bounds__(kLeafThreads, 2)
     k_leaf(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends, const uint32_t* __restrict__ idx,
            const float* __restrict__ pts, int ld, float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
            uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound,
@@ -124,24 +124,22 @@ __global__ void __launch_bounds__(kLeafThreads, MINB)
             __syncthreads();
             distance_block<D>(I, J, Dm);
             __syncthreads();
-            // Each point's 64 offers in column order; the warp's four points
-            // are updated in step with one another.
-            uint32_t cand[kPtsPerWarp][2];
-            float dist[kPtsPerWarp][2];
 #pragma unroll
             for (int u = 0; u < kPtsPerWarp; ++u) {
                 const int row = warp * kPtsPerWarp + u;
                 const uint32_t p = ib + row;
+                if (p < b) {
 #pragma unroll
-                for (int h = 0; h < kBJ / kWarp; ++h) {
-                    const int jj = h * kWarp + lane;
-                    const uint32_t j = jb + jj;
-                    const bool valid = p < b && j < b && j != p;
-                    dist[u][h] = valid ? Dm[row * kDmStride + jj] : __int_as_float(0x7f800000);
-                    cand[u][h] = valid ? ids[j] : 0u;
+                    for (int h = 0; h < kBJ / kWarp; ++h) {
+                        const int jj = h * kWarp + lane;
+                        const uint32_t j = jb + jj;
+                        const bool valid = j < b && j != p;
+                        const float d = Dm[row * kDmStride + jj];
+                        const uint32_t cand = valid ? ids[j] : 0u;
+                        set_offer_batch(sets[u], cand, d, valid, K, lane);
+                    }
                 }
             }
-            set_offer_multi<kPtsPerWarp>(sets, cand, dist, K, lane);
         }
 #pragma unroll
         for (int u = 0; u < kPtsPerWarp; ++u) {
@@ -162,7 +160,7 @@ void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const u
                             static_cast<size_t>(kBI) * kDmStride * sizeof(float) +
                             static_cast<size_t>(std::max<uint32_t>(max_bucket, 1)) * sizeof(uint32_t);
         if (smem > 227 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "bucket too large for the bucket kernel");
-        auto kern = c.leaf_ctas_per_sm == 1 ? k_leaf<D, 1> : k_leaf<D, 2>;
+        auto kern = k_leaf<D>;
         allow_max_smem(c, kern);
         kern<<<count, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
                                                       c.set_id, c.set_size, c.set_maxslot, c.set_bound,

@@ -58,21 +58,30 @@ __global__ void k_iota(uint32_t* __restrict__ idx, uint32_t n) {
 // and the first lloyd_len[i] to its Lloyd list (both CSR).
 // Node [start, end) of a set starting at `base` draws with keys relative to
 // the set, so a set's tree is the same alone and in a batch.
+// With `dcount` the nodes are [0, *dcount) (a grid-stride loop) and seed / rep
+// come from rep_params[0] / [1]; else one node per CTA.
 __global__ void k_draw_positions(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,
                                  const uint32_t* __restrict__ bases, const uint32_t* __restrict__ attempts,
                                  const uint64_t* __restrict__ draw_off,
                                  const uint64_t* __restrict__ seed_off, const uint64_t* __restrict__ lloyd_off,
                                  uint64_t seed, uint32_t rep, uint32_t* __restrict__ seeds_out,
-                                 uint32_t* __restrict__ lloyd_out) {
-    const uint32_t node = blockIdx.x;
-    const uint64_t cnt = draw_off[node + 1] - draw_off[node];
-    const uint64_t sb = seed_off[node], sl = seed_off[node + 1] - sb;
-    const uint64_t lb = lloyd_off[node], ll = lloyd_off[node + 1] - lb;
-    const uint32_t s = starts[node], t = ends[node], a = attempts[node], b = bases[node];
-    for (uint64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-        const uint32_t pos = b + counter_position(seed, rep, s - b, t - b, a, static_cast<uint32_t>(i));
-        if (i < sl) seeds_out[sb + i] = pos;
-        if (i < ll) lloyd_out[lb + i] = pos;
+                                 uint32_t* __restrict__ lloyd_out, const uint32_t* __restrict__ dcount,
+                                 const uint64_t* __restrict__ rep_params) {
+    const uint32_t count = dcount ? *dcount : gridDim.x;
+    if (rep_params) {
+        seed = rep_params[0];
+        rep = static_cast<uint32_t>(rep_params[1]);
+    }
+    for (uint32_t node = blockIdx.x; node < count; node += gridDim.x) {
+        const uint64_t cnt = draw_off[node + 1] - draw_off[node];
+        const uint64_t sb = seed_off[node], sl = seed_off[node + 1] - sb;
+        const uint64_t lb = lloyd_off[node], ll = lloyd_off[node + 1] - lb;
+        const uint32_t s = starts[node], t = ends[node], a = attempts[node], b = bases[node];
+        for (uint64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            const uint32_t pos = b + counter_position(seed, rep, s - b, t - b, a, static_cast<uint32_t>(i));
+            if (i < sl) seeds_out[sb + i] = pos;
+            if (i < ll) lloyd_out[lb + i] = pos;
+        }
     }
 }
 
@@ -96,10 +105,14 @@ template <int D>
 __global__ void k_farthest_pair(const uint64_t* __restrict__ offsets, const uint32_t* __restrict__ positions,
                                 const uint32_t* __restrict__ idx, const float* __restrict__ pts, int ld,
                                 uint32_t* __restrict__ out_first, uint32_t* __restrict__ out_second,
-                                int32_t* __restrict__ out_ok, float* __restrict__ c1, float* __restrict__ c2) {
+                                int32_t* __restrict__ out_ok, float* __restrict__ c1, float* __restrict__ c2,
+                                const uint32_t* __restrict__ dcount) {
     extern __shared__ float4 smem4[];
     float* rows = reinterpret_cast<float*>(smem4);
-    const uint32_t node = blockIdx.x;
+    __shared__ float sv[kPairThreads / kWarp];
+    __shared__ uint32_t si[kPairThreads / kWarp], sj[kPairThreads / kWarp];
+    const uint32_t count = dcount ? *dcount : gridDim.x;
+    for (uint32_t node = blockIdx.x; node < count; node += gridDim.x) {
     const uint64_t b = offsets[node];
     const uint32_t m = static_cast<uint32_t>(offsets[node + 1] - b);
     constexpr int Q = (D + 3) / 4;
@@ -124,8 +137,6 @@ __global__ void k_farthest_pair(const uint64_t* __restrict__ offsets, const uint
         }
     }
     // Block arg-max: larger distance wins; equal distances -> smaller (i, j).
-    __shared__ float sv[kPairThreads / kWarp];
-    __shared__ uint32_t si[kPairThreads / kWarp], sj[kPairThreads / kWarp];
     auto better = [](float v, uint32_t i, uint32_t j, float bv, uint32_t bi2, uint32_t bj2) {
         if (i == kNone) return false;
         if (bi2 == kNone) return true;
@@ -170,17 +181,20 @@ __global__ void k_farthest_pair(const uint64_t* __restrict__ offsets, const uint
         c1[static_cast<size_t>(node) * ld + q] = bi != kNone ? rows[bi * Q * 4 + q] : 0.0f;
         c2[static_cast<size_t>(node) * ld + q] = bj != kNone ? rows[bj * Q * 4 + q] : 0.0f;
     }
+    __syncthreads();  // rows and the arg-max slots are reused by the next node
+    }
 }
 
 // between = 0.5f * (c1 + c2); coefs = c1 - between; offset = dot(between, coefs).
 template <int D>
 __global__ void k_plane(const float* __restrict__ c1, const float* __restrict__ c2, int ld, uint32_t count,
-                        float* __restrict__ coefs, float* __restrict__ offsets) {
-    const uint32_t node = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+                        float* __restrict__ coefs, float* __restrict__ offsets, const uint32_t* __restrict__ dcount) {
+    if (dcount) count = *dcount;
     const int lane = threadIdx.x % kWarp;
-    if (node >= count) return;
     __shared__ float between_s[8][(D + 3) / 4 * 4];
     float* between = between_s[threadIdx.x / kWarp];
+    for (uint32_t node = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp; node < count;
+         node += gridDim.x * (blockDim.x / kWarp)) {
     const size_t base = static_cast<size_t>(node) * ld;
     for (int j = lane; j < ld; j += kWarp) {
         if (j < D) {
@@ -193,6 +207,8 @@ __global__ void k_plane(const float* __restrict__ c1, const float* __restrict__ 
     }
     __syncwarp();
     if (lane == 0) offsets[node] = canonical_dot<D>(between, coefs + base);
+    __syncwarp();
+    }
 }
 
 // ------------------------------------------------------------ side test
@@ -254,9 +270,12 @@ __global__ void __launch_bounds__(kSideThreads) k_side(const Item* __restrict__ 
                                                        int ld, const float* __restrict__ coefs,
                                                        const float* __restrict__ offsets, uint8_t* __restrict__ flags,
                                                        uint32_t* __restrict__ ids_out,
-                                                       uint32_t* __restrict__ item_true) {
+                                                       uint32_t* __restrict__ item_true,
+                                                       const uint32_t* __restrict__ dcount) {
     __shared__ uint32_t warp_sum[kSideThreads / kWarp];
-    const Item it = items[blockIdx.x];
+    const uint32_t n_items = dcount ? *dcount : gridDim.x;
+    for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const Item it = items[item];
     const bool from_list = (it.node & kListItem) != 0;
     const uint32_t node = it.node & ~kListItem;
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
@@ -296,7 +315,9 @@ __global__ void __launch_bounds__(kSideThreads) k_side(const Item* __restrict__ 
     if (threadIdx.x == 0) {
         uint32_t s = 0;
         for (int w = 0; w < kSideThreads / kWarp; ++w) s += warp_sum[w];
-        item_true[blockIdx.x] = s;
+        item_true[item] = s;
+    }
+    __syncthreads();  // warp_sum is reused by the next item
     }
 }
 
@@ -331,15 +352,16 @@ __global__ void __launch_bounds__(kSeqThreads) k_lloyd_seq(const SeqNode* __rest
                                                            const uint32_t* __restrict__ ids,
                                                            const float* __restrict__ pts, int ld, float* __restrict__ c1,
                                                            float* __restrict__ c2, int32_t* __restrict__ ok,
-                                                           int32_t* __restrict__ error_flag) {
+                                                           int32_t* __restrict__ error_flag,
+                                                           const uint32_t* __restrict__ dcount) {
     extern __shared__ __align__(128) unsigned char smem[];
     float* tiles = reinterpret_cast<float*>(smem);                                   // [stage][row][D]
     uint8_t* tflags = smem + static_cast<size_t>(kSeqStages) * kSeqRows * D * 4;  // [stage][row]
     __shared__ uint64_t full[kSeqStages], empty[kSeqStages];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
-    const uint32_t node = blockIdx.x;
-    const SeqNode nd = nodes[node];
-    const uint32_t ntiles = (nd.len + kSeqRows - 1) / kSeqRows;
+    // Nodes blockIdx.x, blockIdx.x + gridDim.x, ... of [0, count); their
+    // tiles run through one ring, tile g of the CTA in stage g % kSeqStages.
+    const uint32_t count = dcount ? *dcount : gridDim.x;
     if (threadIdx.x == 0) {
         for (int s = 0; s < kSeqStages; ++s) {
             tc::mbar_init(&full[s], 1);
@@ -350,93 +372,102 @@ __global__ void __launch_bounds__(kSeqThreads) k_lloyd_seq(const SeqNode* __rest
     __syncthreads();
     constexpr uint32_t kRowBytes = D * sizeof(float);
     if (warp == 2) {
-        // Producer: ids of the next tile are loaded while this one is issued.
-        uint32_t next[kSeqRows / kWarp];
-        auto load_ids = [&](uint32_t t) {
+        // Producer: a node's ids of the next tile are loaded while this one is issued.
+        uint32_t g = 0;
+        bool failed = false;
+        for (uint32_t node = blockIdx.x; node < count && !failed; node += gridDim.x) {
+            const SeqNode nd = nodes[node];
+            const uint32_t ntiles = (nd.len + kSeqRows - 1) / kSeqRows;
+            uint32_t next[kSeqRows / kWarp];
+            auto load_ids = [&](uint32_t t) {
 #pragma unroll
-            for (int u = 0; u < kSeqRows / kWarp; ++u) {
-                const uint32_t e = t * kSeqRows + lane + u * kWarp;
-                next[u] = (t < ntiles && e < nd.len) ? ids[nd.fbase + e] : 0u;
-            }
-        };
-        load_ids(0);
-        uint32_t issued = 0;
-        for (uint32_t t = 0; t < ntiles; ++t) {
-            uint32_t cur[kSeqRows / kWarp];
+                for (int u = 0; u < kSeqRows / kWarp; ++u) {
+                    const uint32_t e = t * kSeqRows + lane + u * kWarp;
+                    next[u] = (t < ntiles && e < nd.len) ? ids[nd.fbase + e] : 0u;
+                }
+            };
+            load_ids(0);
+            for (uint32_t t = 0; t < ntiles; ++t, ++g) {
+                uint32_t cur[kSeqRows / kWarp];
 #pragma unroll
-            for (int u = 0; u < kSeqRows / kWarp; ++u) cur[u] = next[u];
-            load_ids(t + 1);
-            const uint32_t s = t % kSeqStages;
-            if (t >= kSeqStages && !tc::mbar_wait_limited(&empty[s], ((t / kSeqStages) - 1) & 1u)) {
-                if (lane == 0) atomicExch(error_flag, 1);
-                break;
-            }
-            const uint32_t rows = min(static_cast<uint32_t>(kSeqRows), nd.len - t * kSeqRows);
-            const uint32_t fbytes = (rows + 15u) & ~15u;
-            if (lane == 0) tc::mbar_arrive_expect_tx(&full[s], rows * kRowBytes + fbytes);
-            __syncwarp();
+                for (int u = 0; u < kSeqRows / kWarp; ++u) cur[u] = next[u];
+                load_ids(t + 1);
+                const uint32_t s = g % kSeqStages;
+                if (g >= kSeqStages && !tc::mbar_wait_limited(&empty[s], ((g / kSeqStages) - 1) & 1u)) {
+                    if (lane == 0) atomicExch(error_flag, 1);
+                    failed = true;
+                    break;
+                }
+                const uint32_t rows = min(static_cast<uint32_t>(kSeqRows), nd.len - t * kSeqRows);
+                const uint32_t fbytes = (rows + 15u) & ~15u;
+                if (lane == 0) tc::mbar_arrive_expect_tx(&full[s], rows * kRowBytes + fbytes);
+                __syncwarp();
 #pragma unroll
-            for (int u = 0; u < kSeqRows / kWarp; ++u) {
-                const uint32_t r = lane + u * kWarp;
-                if (r < rows)
-                    tc::bulk_g2s(tiles + (static_cast<size_t>(s) * kSeqRows + r) * D,
-                                 pts + static_cast<size_t>(cur[u]) * ld, kRowBytes, &full[s]);
+                for (int u = 0; u < kSeqRows / kWarp; ++u) {
+                    const uint32_t r = lane + u * kWarp;
+                    if (r < rows)
+                        tc::bulk_g2s(tiles + (static_cast<size_t>(s) * kSeqRows + r) * D,
+                                     pts + static_cast<size_t>(cur[u]) * ld, kRowBytes, &full[s]);
+                }
+                if (lane == 0) tc::bulk_g2s(tflags + s * kSeqRows, flags + nd.fbase + t * kSeqRows, fbytes, &full[s]);
             }
-            if (lane == 0) tc::bulk_g2s(tflags + s * kSeqRows, flags + nd.fbase + t * kSeqRows, fbytes, &full[s]);
-            issued = t + 1;
         }
         // No copy may be in flight when the CTA exits.
-        const uint32_t first = issued > kSeqStages ? issued - kSeqStages : 0u;
-        for (uint32_t t = first; t < issued; ++t)
+        const uint32_t first = g > kSeqStages ? g - kSeqStages : 0u;
+        for (uint32_t t = first; t < g; ++t)
             if (!tc::mbar_wait(&full[t % kSeqStages], (t / kSeqStages) & 1u) && lane == 0) atomicExch(error_flag, 1);
         return;
     }
     // Consumers: warp 0 sums the side-true rows, warp 1 the side-false rows.
     const uint8_t want = warp == 0 ? 1 : 0;
     constexpr int PER = (D + kWarp - 1) / kWarp;
-    double acc[PER];
+    uint32_t g = 0;
+    for (uint32_t node = blockIdx.x; node < count; node += gridDim.x) {
+        const SeqNode nd = nodes[node];
+        const uint32_t ntiles = (nd.len + kSeqRows - 1) / kSeqRows;
+        double acc[PER];
 #pragma unroll
-    for (int j = 0; j < PER; ++j) acc[j] = 0.0;
-    uint32_t cnt = 0;
-    bool healthy = true;
-    for (uint32_t t = 0; t < ntiles; ++t) {
-        const uint32_t s = t % kSeqStages;
-        if (!tc::mbar_wait_limited(&full[s], (t / kSeqStages) & 1u)) {
-            if (lane == 0) atomicExch(error_flag, 1);
-            healthy = false;
-            break;
-        }
-        const uint32_t rows = min(static_cast<uint32_t>(kSeqRows), nd.len - t * kSeqRows);
-        const float* tile = tiles + static_cast<size_t>(s) * kSeqRows * D;
-        const uint8_t* tf = tflags + s * kSeqRows;
-#pragma unroll 4
-        for (uint32_t r = 0; r < rows; ++r) {
-            if (tf[r] == want) {
-#pragma unroll
-                for (int j = 0; j < PER; ++j)
-                    if (lane + j * kWarp < D)
-                        acc[j] = __dadd_rn(acc[j], static_cast<double>(tile[r * D + lane + j * kWarp]));
-                ++cnt;
+        for (int j = 0; j < PER; ++j) acc[j] = 0.0;
+        uint32_t cnt = 0;
+        for (uint32_t t = 0; t < ntiles; ++t, ++g) {
+            const uint32_t s = g % kSeqStages;
+            if (!tc::mbar_wait_limited(&full[s], (g / kSeqStages) & 1u)) {
+                if (lane == 0) atomicExch(error_flag, 1);
+                return;
             }
-        }
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive(&empty[s]);
-    }
-    if (!healthy) return;
-    if (cnt == 0) {
-        if (lane == 0) ok[node] = 0;
-        return;
-    }
-    float* c = (warp == 0 ? c1 : c2) + static_cast<size_t>(node) * ld;
-    const double nn = static_cast<double>(cnt);
+            const uint32_t rows = min(static_cast<uint32_t>(kSeqRows), nd.len - t * kSeqRows);
+            const float* tile = tiles + static_cast<size_t>(s) * kSeqRows * D;
+            const uint8_t* tf = tflags + s * kSeqRows;
+#pragma unroll 4
+            for (uint32_t r = 0; r < rows; ++r) {
+                if (tf[r] == want) {
 #pragma unroll
-    for (int j = 0; j < PER; ++j)
-        if (lane + j * kWarp < D) c[lane + j * kWarp] = __double2float_rn(__ddiv_rn(acc[j], nn));
+                    for (int j = 0; j < PER; ++j)
+                        if (lane + j * kWarp < D)
+                            acc[j] = __dadd_rn(acc[j], static_cast<double>(tile[r * D + lane + j * kWarp]));
+                    ++cnt;
+                }
+            }
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&empty[s]);
+        }
+        if (cnt == 0) {
+            if (lane == 0) ok[node] = 0;
+            continue;
+        }
+        float* c = (warp == 0 ? c1 : c2) + static_cast<size_t>(node) * ld;
+        const double nn = static_cast<double>(cnt);
+#pragma unroll
+        for (int j = 0; j < PER; ++j)
+            if (lane + j * kWarp < D) c[lane + j * kWarp] = __double2float_rn(__ddiv_rn(acc[j], nn));
+    }
 }
 
 // Exclusive scan of n values into out[0..n] (out[n] = total); one CTA.
-__global__ void k_scan_items(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ out) {
+__global__ void k_scan_items(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ out,
+                             const uint32_t* __restrict__ dn) {
     __shared__ uint32_t part[1024];
+    if (dn) n = *dn;
     const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
     const uint32_t b = threadIdx.x * per, e = min(n, b + per);
     uint32_t s = 0;
@@ -461,9 +492,11 @@ __global__ void k_scan_items(const uint32_t* __restrict__ in, uint32_t n, uint32
 }
 
 __global__ void k_node_true(const uint32_t* __restrict__ item_begin, const uint32_t* __restrict__ item_end,
-                            const uint32_t* __restrict__ prefix, uint32_t count, uint32_t* __restrict__ out_true) {
-    const uint32_t node = blockIdx.x * blockDim.x + threadIdx.x;
-    if (node < count) out_true[node] = prefix[item_end[node]] - prefix[item_begin[node]];
+                            const uint32_t* __restrict__ prefix, uint32_t count, uint32_t* __restrict__ out_true,
+                            const uint32_t* __restrict__ dcount) {
+    if (dcount) count = *dcount;
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < count; node += gridDim.x * blockDim.x)
+        out_true[node] = prefix[item_end[node]] - prefix[item_begin[node]];
 }
 
 // Stable partition scatter of one chunk: side-true positions go to
@@ -475,12 +508,15 @@ __global__ void __launch_bounds__(kSideThreads) k_scatter(const Item* __restrict
                                                           const uint32_t* __restrict__ prefix,
                                                           const uint8_t* __restrict__ flags,
                                                           const uint32_t* __restrict__ idx,
-                                                          uint32_t* __restrict__ idx_out) {
+                                                          uint32_t* __restrict__ idx_out,
+                                                          const uint32_t* __restrict__ dcount) {
     __shared__ uint32_t warp_tot[kSideThreads / kWarp];
-    const Item it = items[blockIdx.x];
+    const uint32_t n_items = dcount ? *dcount : gridDim.x;
+    for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const Item it = items[item];
     const uint32_t s = node_start[it.node];
     const uint32_t T = node_true[it.node];
-    const uint32_t before_item = prefix[blockIdx.x] - prefix[node_item_begin[it.node]];
+    const uint32_t before_item = prefix[item] - prefix[node_item_begin[it.node]];
     // Thread t owns positions [t*kSidePer, (t+1)*kSidePer) of the chunk.
     const uint32_t first = threadIdx.x * kSidePer;
     uint8_t f[kSidePer];
@@ -520,12 +556,17 @@ __global__ void __launch_bounds__(kSideThreads) k_scatter(const Item* __restrict
             idx_out[dst] = idx[pos];
         }
     }
+    __syncthreads();  // warp_tot is reused by the next item
+    }
 }
 
 __global__ void k_copy_back(const Item* __restrict__ items, const uint32_t* __restrict__ src,
-                            uint32_t* __restrict__ dst) {
-    const Item it = items[blockIdx.x];
-    for (uint32_t r = threadIdx.x; r < it.count; r += blockDim.x) dst[it.begin + r] = src[it.begin + r];
+                            uint32_t* __restrict__ dst, const uint32_t* __restrict__ dcount) {
+    const uint32_t n_items = dcount ? *dcount : gridDim.x;
+    for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const Item it = items[item];
+        for (uint32_t r = threadIdx.x; r < it.count; r += blockDim.x) dst[it.begin + r] = src[it.begin + r];
+    }
 }
 
 }  // namespace
@@ -545,7 +586,7 @@ void launch_draw_positions(Context& c, uint32_t count, const uint32_t* d_starts,
                            uint32_t* d_seeds, uint32_t* d_lloyd) {
     if (count == 0) return;
     k_draw_positions<<<count, 256, 0, c.stream>>>(d_starts, d_ends, d_bases, d_attempts, d_draw_off, d_seed_off, d_lloyd_off,
-                                                  seed, rep, d_seeds, d_lloyd);
+                                                  seed, rep, d_seeds, d_lloyd, nullptr, nullptr);
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
 }
@@ -568,7 +609,7 @@ void launch_farthest_pair(Context& c, uint32_t count, const uint64_t* d_offsets,
         auto kern = k_farthest_pair<D>;
         allow_max_smem(c, kern);
         kern<<<count, kPairThreads, smem, c.stream>>>(d_offsets, d_positions, c.indices, c.points, c.ld, d_first,
-                                                      d_second, d_ok, d_c1, d_c2);
+                                                      d_second, d_ok, d_c1, d_c2, nullptr);
     });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
@@ -578,7 +619,7 @@ void launch_plane(Context& c, uint32_t count, const float* d_c1, const float* d_
                   float* d_offsets) {
     if (count == 0) return;
     KNNG_DISPATCH_D(c.d, {
-        k_plane<D><<<(count + 7) / 8, 256, 0, c.stream>>>(d_c1, d_c2, c.ld, count, d_coefs, d_offsets);
+        k_plane<D><<<(count + 7) / 8, 256, 0, c.stream>>>(d_c1, d_c2, c.ld, count, d_coefs, d_offsets, nullptr);
     });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
@@ -620,9 +661,9 @@ void launch_lloyd(Context& c, uint32_t count, const uint32_t* h_starts, const ui
         for (uint32_t iter = 0; iter < iters; ++iter) {
             launch_plane(c, count, d_c1, d_c2, d_coefs, d_offsets);
             k_side<D><<<ni, kSideThreads, 0, c.stream>>>(d_items, d_lloyd_positions, c.indices, c.points, c.ld,
-                                                         d_coefs, d_offsets, flags, ids, item_true);
+                                                         d_coefs, d_offsets, flags, ids, item_true, nullptr);
             seq<<<count, kSeqThreads, seq_smem_bytes(D), c.stream>>>(d_nodes, flags, ids, c.points, c.ld, d_c1, d_c2,
-                                                                     d_ok, err);
+                                                                     d_ok, err, nullptr);
             c.launches += 2;
             KNNG_CUDA(cudaGetLastError());
         }
@@ -650,13 +691,13 @@ void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, cons
     uint32_t* prefix = static_cast<uint32_t*>(scratch(c, "item_prefix", (ni + 1) * sizeof(uint32_t)));
     KNNG_DISPATCH_D(c.d, {
         k_side<D><<<ni, kSideThreads, 0, c.stream>>>(d_items, nullptr, c.indices, c.points, c.ld, d_coefs, d_offsets,
-                                                     flags, nullptr, item_true);
+                                                     flags, nullptr, item_true, nullptr);
     });
-    k_scan_items<<<1, 1024, 0, c.stream>>>(item_true, ni, prefix);
-    k_node_true<<<(count + 255) / 256, 256, 0, c.stream>>>(d_ib, d_ie, prefix, count, d_true);
+    k_scan_items<<<1, 1024, 0, c.stream>>>(item_true, ni, prefix, nullptr);
+    k_node_true<<<(count + 255) / 256, 256, 0, c.stream>>>(d_ib, d_ie, prefix, count, d_true, nullptr);
     k_scatter<<<ni, kSideThreads, 0, c.stream>>>(d_items, d_starts, d_ib, d_true, prefix, flags, c.indices,
-                                                 c.indices_tmp);
-    k_copy_back<<<ni, 256, 0, c.stream>>>(d_items, c.indices_tmp, c.indices);
+                                                 c.indices_tmp, nullptr);
+    k_copy_back<<<ni, 256, 0, c.stream>>>(d_items, c.indices_tmp, c.indices, nullptr);
     c.launches += 5;
     KNNG_CUDA(cudaGetLastError());
 }
