@@ -85,6 +85,18 @@ void* scratch(Context& c, const char* name, size_t bytes) {
     return b.ptr;
 }
 
+// --------------------------------------------------------------- sizing rules
+
+// getSampleFromPercent's sample size: (uint32)(n * (float)((ln n / ln 30)^7 / n))
+// (src/SolutionKmeans.hpp:50-58).
+uint32_t sample_count(uint32_t n) {
+    const float frac = static_cast<float>(std::pow(std::log(static_cast<double>(n)) / std::log(30.0), 7) / n);
+    return static_cast<uint32_t>(static_cast<float>(n) * frac);
+}
+
+// kmeansStartVecs' seed count: (uint32)(log10 n)^2.5 (src/SolutionKmeans.hpp:70, :105).
+uint32_t start_count(uint32_t n) { return static_cast<uint32_t>(std::pow(std::log10(static_cast<double>(n)), 2.5)); }
+
 void* staging_take(Context& c, size_t bytes) {
     bytes = (bytes + 15) / 16 * 16;
     if (bytes > c.staging_cap) {
@@ -144,6 +156,7 @@ void free_sets(Context& c) {
 
 void release_all(Context& c) {
     if (c.stream) cudaStreamSynchronize(c.stream);
+    devrep_release(c);
     free_points(c);
     free_sets(c);
     dev_free(c, c.indices, c.n * sizeof(uint32_t));
@@ -156,17 +169,6 @@ void release_all(Context& c) {
 
 namespace {
 
-// --------------------------------------------------------------- sizing rules
-
-// getSampleFromPercent's sample size: (uint32)(n * (float)((ln n / ln 30)^7 / n))
-// (src/SolutionKmeans.hpp:50-58).
-uint32_t sample_count(uint32_t n) {
-    const float frac = static_cast<float>(std::pow(std::log(static_cast<double>(n)) / std::log(30.0), 7) / n);
-    return static_cast<uint32_t>(static_cast<float>(n) * frac);
-}
-
-// kmeansStartVecs' seed count: (uint32)(log10 n)^2.5 (src/SolutionKmeans.hpp:70, :105).
-uint32_t start_count(uint32_t n) { return static_cast<uint32_t>(std::pow(std::log10(static_cast<double>(n)), 2.5)); }
 
 struct EventPair {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -400,6 +402,34 @@ void run_rep(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small
              uint32_t rep, RepStats& st, knng_stats* stats, uint32_t precision = KNNG_PRECISION_FP32) {
     require_sets(c);
     if (max_leaf < 2) fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be >= 2");
+    if (c.rep_loop != 2) {
+        // Device-side levels (one graph, or level by level), then the bucket
+        // pass over the device's leaf list.
+        DevRepResult res;
+        run_rep_device(c, max_leaf, lloyd_iters, small_threshold, seed, rep, precision, c.rep_loop == 0, res);
+        std::vector<std::pair<uint32_t, uint32_t>> lv(res.leaf_start.size());
+        for (size_t i = 0; i < lv.size(); ++i) lv[i] = {res.leaf_start[i], res.leaf_end[i]};
+        std::sort(lv.begin(), lv.end());
+        c.last_leaf_start.resize(lv.size());
+        c.last_leaf_end.resize(lv.size());
+        for (size_t i = 0; i < lv.size(); ++i) {
+            c.last_leaf_start[i] = lv[i].first;
+            c.last_leaf_end[i] = lv[i].second;
+        }
+        st.levels += res.levels;
+        st.nodes += res.nodes;
+        st.restarts += res.restarts;
+        st.fallbacks += res.fallbacks;
+        st.ms_split += res.ms_split;
+        st.ms_leaf += res.ms_leaf;
+        if (stats) {
+            stats->buckets += lv.size();
+            stats->bucket_pairs += res.pairs;
+            stats->leaf_launches += 1;
+            stats->ms_leaf_kernel += res.ms_leaf;
+        }
+        return;
+    }
     EventPair split_t(c);
     launch_iota(c);
     std::vector<Node> level;
@@ -609,6 +639,9 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     if (const char* r = std::getenv("KNNG_REFINE")) c->refine_mode = std::strcmp(r, "pointwise") == 0 ? 1 : 0;
     if (const char* r = std::getenv("KNNG_REFINE_SLOTS")) c->refine_slots = std::max(0, std::atoi(r));
     if (const char* r = std::getenv("KNNG_JOIN_ORDER")) c->join_order_ids = std::strcmp(r, "id") == 0;
+    if (const char* r = std::getenv("KNNG_REP_LOOP"))
+        c->rep_loop = std::strcmp(r, "host") == 0 ? 2 : (std::strcmp(r, "device") == 0 ? 1 : 0);
+    c->sms = prop.multiProcessorCount;
     if (const char* r = std::getenv("KNNG_REFINE_POOL")) c->refine_pool = std::max<long long>(0, std::atoll(r));
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {

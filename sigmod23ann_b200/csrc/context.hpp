@@ -33,6 +33,8 @@ struct Timer {
     cudaEvent_t start = nullptr, stop = nullptr;
 };
 
+struct DevRep;  // buffers and graphs of the device-side repetition (split.cu)
+
 struct Context {
     int device = 0;
     uint64_t budget = 0;
@@ -70,6 +72,16 @@ struct Context {
     std::vector<std::pair<std::string, DeviceBuffer>> scratch;
 
     uint64_t launches = 0;
+
+    // How a repetition's tree is built: 0 = one CUDA graph per repetition
+    // (device-side levels under a WHILE node, the default), 1 = the same
+    // device-side levels launched one by one, 2 = levels sequenced by the
+    // host (environment KNNG_REP_LOOP=graph|device|host at creation).
+    int rep_loop = 0;
+    DevRep* devrep = nullptr;
+    // Set while a graph is being captured: no attribute or allocation calls.
+    bool capturing = false;
+    int sms = 148;
 
     // Pinned host staging for small transfers: an upload is copied here and
     // sent asynchronously, a download lands here first; the space is reused
@@ -151,6 +163,7 @@ bool dim_supported(uint32_t d);
 // passes its own size).
 template <class Kernel>
 void allow_max_smem(Context& c, Kernel kern) {
+    if (c.capturing) return;  // set before the capture began
     int optin = 0;
     KNNG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
     cudaFuncAttributes fa{};
@@ -187,9 +200,32 @@ void launch_lloyd(Context& c, uint32_t count, const uint32_t* h_starts, const ui
 // the number of side-true points of node i.
 void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, const uint32_t* h_ends,
                       const uint32_t* d_starts, const float* d_coefs, const float* d_offsets, uint32_t* d_true);
+// Device-side repetition (split.cu): the tree built by device-side levels,
+// as one CUDA graph (graph = true) or launched level by level, then the
+// bucket pass over the device's leaf list.
+struct DevRepResult {
+    std::vector<uint32_t> leaf_start, leaf_end;  // in no particular order
+    double ms_split = 0, ms_leaf = 0;
+    uint64_t levels = 0, nodes = 0, restarts = 0, fallbacks = 0, pairs = 0;
+};
+void run_rep_device(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold, uint64_t seed,
+                    uint32_t rep, uint32_t precision, bool graph, DevRepResult& out);
+void devrep_release(Context& c);
+// Sizing rules of the sampling plan (getSampleFromPercent, kmeansStartVecs).
+uint32_t sample_count(uint32_t n);
+uint32_t start_count(uint32_t n);
 // leaf.cu
 void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
                    uint32_t max_bucket, uint64_t* evals);
+// Persistent bucket pass over a device list of *d_count buckets taken from
+// the work counter *d_work (zeroed beforehand).
+void launch_leaves_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
+                        uint32_t* d_work, uint32_t max_bucket);
+void launch_leaves_bf16_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
+                             uint32_t* d_work, uint32_t* d_error);
+// Kernel attributes of the two list launchers, set before a graph capture.
+void prepare_leaves_list(Context& c);
+void prepare_leaves_bf16_list(Context& c);
 // leaf_bf16.cu: the precision form (BF16 tensor-core estimates, the 128 best
 // candidates per point re-ranked in FP32), buckets of at most 512 points.
 void launch_leaves_bf16(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,

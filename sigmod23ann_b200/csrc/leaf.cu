@@ -98,18 +98,33 @@ __global__ void __launch_bounds__(kLeafThreads, 2)
     k_leaf(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends, const uint32_t* __restrict__ idx,
            const float* __restrict__ pts, int ld, float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
            uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot, float* __restrict__ set_bound,
-           int K) {
+           int K, const uint32_t* __restrict__ dcount, uint32_t* __restrict__ work) {
     extern __shared__ float4 smem4[];
     float* I = reinterpret_cast<float*>(smem4);
     float* J = I + D * kBI;
     float* Dm = J + D * kBJ;
     uint32_t* ids = reinterpret_cast<uint32_t*>(Dm + kBI * kDmStride);
-    const uint32_t s = starts[blockIdx.x];
-    const uint32_t b = ends[blockIdx.x] - s;
-    if (b < 2) return;
+    __shared__ uint32_t next_s;
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    // One bucket per CTA, or (with `work`) buckets [0, *dcount) taken one at a
+    // time from the work counter by a persistent grid.
+    for (uint32_t round = 0;; ++round) {
+    uint32_t leaf;
+    if (work) {
+        if (threadIdx.x == 0) next_s = atomicAdd(work, 1u);
+        __syncthreads();
+        leaf = next_s;
+        __syncthreads();
+        if (leaf >= *dcount) break;
+    } else {
+        if (round > 0) break;
+        leaf = blockIdx.x;
+    }
+    const uint32_t s = starts[leaf];
+    const uint32_t b = ends[leaf] - s;
+    if (b < 2) continue;
     for (uint32_t t = threadIdx.x; t < b; t += kLeafThreads) ids[t] = idx[s + t];
     __syncthreads();
-    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     for (uint32_t ib = 0; ib < b; ib += kBI) {
         load_tile<D>(I, ids, ib, b, pts, ld);
         WarpSet sets[kPtsPerWarp];
@@ -148,6 +163,7 @@ __global__ void __launch_bounds__(kLeafThreads, 2)
         }
         __syncthreads();  // everyone is done with I before it is reloaded
     }
+    }
 }
 
 }  // namespace
@@ -164,11 +180,34 @@ void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const u
         allow_max_smem(c, kern);
         kern<<<count, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
                                                       c.set_id, c.set_size, c.set_maxslot, c.set_bound,
-                                                      static_cast<int>(c.k));
+                                                      static_cast<int>(c.k), nullptr, nullptr);
     });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     (void)evals;
+}
+
+void prepare_leaves_list(Context& c) {
+    KNNG_DISPATCH_D(c.d, { allow_max_smem(c, k_leaf<D>); });
+}
+
+void launch_leaves_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
+                        uint32_t* d_work, uint32_t max_bucket) {
+    KNNG_DISPATCH_D(c.d, {
+        const size_t smem = static_cast<size_t>(D) * (kBI + kBJ) * sizeof(float) +
+                            static_cast<size_t>(kBI) * kDmStride * sizeof(float) +
+                            static_cast<size_t>(std::max<uint32_t>(max_bucket, 1)) * sizeof(uint32_t);
+        if (smem > 227 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "bucket too large for the bucket kernel");
+        auto kern = k_leaf<D>;
+        allow_max_smem(c, kern);
+        const int sms = c.sms;
+        // Persistent: two CTAs per SM take the buckets from the work counter.
+        kern<<<2 * sms, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
+                                                        c.set_id, c.set_size, c.set_maxslot, c.set_bound,
+                                                        static_cast<int>(c.k), d_count, d_work);
+    });
+    ++c.launches;
+    KNNG_CUDA(cudaGetLastError());
 }
 
 }  // namespace knng

@@ -132,7 +132,8 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     k_leaf_bf16(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,
                 const uint32_t* __restrict__ idx, const float* __restrict__ pts, int ld, float* __restrict__ set_dist,
                 uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
-                float* __restrict__ set_bound, int K, uint32_t* __restrict__ error_flag) {
+                float* __restrict__ set_bound, int K, uint32_t* __restrict__ error_flag,
+                const uint32_t* __restrict__ dcount, uint32_t* __restrict__ work) {
     using L = BfLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* A = smem + L::a;
@@ -144,11 +145,8 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     uint32_t* ids = reinterpret_cast<uint32_t*>(smem + L::ids);
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
-    const uint32_t s0 = starts[blockIdx.x];
-    const uint32_t b = ends[blockIdx.x] - s0;
-    if (b < 2) return;
+    __shared__ uint32_t next_s;
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
-    for (uint32_t t = tid; t < b; t += kBfThreads) ids[t] = idx[s0 + t];
     if (warp == 0) tc::tmem_alloc(&tmem_slot, kBfCols);
     if (tid == 0) {
         tc::mbar_init(&mbar, 1);
@@ -158,12 +156,31 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    for (int k = tid; k < D; k += kBfThreads) centre[k] = pts[static_cast<size_t>(ids[0]) * ld + k];
-    __syncthreads();
-    for (uint32_t t = tid; t < b; t += kBfThreads) norms[t] = centred_norm<D>(pts, ld, ids[t], centre);
     uint32_t phase = 0;
     bool healthy = true;
     const uint32_t idesc = tc::idesc_bf16(kBfRows, kBfCols);
+    // One bucket per CTA, or (with `work`) buckets [0, *dcount) taken one at a
+    // time from the work counter by a persistent grid.
+    for (uint32_t round = 0; healthy; ++round) {
+    uint32_t leaf;
+    if (work) {
+        if (tid == 0) next_s = atomicAdd(work, 1u);
+        __syncthreads();
+        leaf = next_s;
+        __syncthreads();
+        if (leaf >= *dcount) break;
+    } else {
+        if (round > 0) break;
+        leaf = blockIdx.x;
+    }
+    const uint32_t s0 = starts[leaf];
+    const uint32_t b = ends[leaf] - s0;
+    if (b < 2) continue;
+    for (uint32_t t = tid; t < b; t += kBfThreads) ids[t] = idx[s0 + t];
+    __syncthreads();
+    for (int k = tid; k < D; k += kBfThreads) centre[k] = pts[static_cast<size_t>(ids[0]) * ld + k];
+    __syncthreads();
+    for (uint32_t t = tid; t < b; t += kBfThreads) norms[t] = centred_norm<D>(pts, ld, ids[t], centre);
     const bool keep_all = b - 1 <= static_cast<uint32_t>(kKeep);
     for (uint32_t rb = 0; rb < b && healthy; rb += kBfRows) {
         const uint32_t cnt = min(static_cast<uint32_t>(kBfRows), b - rb);
@@ -266,6 +283,7 @@ __global__ void __launch_bounds__(kBfThreads, 1)
         }
         __syncthreads();
     }
+    }
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
@@ -366,13 +384,34 @@ void launch_leaves_bf16(Context& c, uint32_t count, const uint32_t* d_starts, co
         allow_max_smem(c, kern);
         kern<<<count, kBfThreads, BfLayout<D>::bytes, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld,
                                                                   c.set_dist, c.set_id, c.set_size, c.set_maxslot,
-                                                                  c.set_bound, static_cast<int>(c.k), err);
+                                                                  c.set_bound, static_cast<int>(c.k), err, nullptr,
+                                                                  nullptr);
     });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     uint32_t h = 0;
     download(c, &h, err, 1);
     if (h) fail(KNNG_ERR_CUDA, "BF16 bucket pass: the MMA completion wait gave up");
+}
+
+void prepare_leaves_bf16_list(Context& c) {
+    KNNG_DISPATCH_D(c.d, { allow_max_smem(c, k_leaf_bf16<D>); });
+}
+
+void launch_leaves_bf16_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
+                             uint32_t* d_work, uint32_t* d_error) {
+    const int sms = c.sms;
+    KNNG_DISPATCH_D(c.d, {
+        auto kern = k_leaf_bf16<D>;
+        allow_max_smem(c, kern);
+        // Persistent: one CTA per SM takes the buckets from the work counter.
+        kern<<<sms, kBfThreads, BfLayout<D>::bytes, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld,
+                                                                c.set_dist, c.set_id, c.set_size, c.set_maxslot,
+                                                                c.set_bound, static_cast<int>(c.k), d_error, d_count,
+                                                                d_work);
+    });
+    ++c.launches;
+    KNNG_CUDA(cudaGetLastError());
 }
 
 }  // namespace knng

@@ -24,6 +24,9 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -569,6 +572,300 @@ __global__ void k_copy_back(const Item* __restrict__ items, const uint32_t* __re
     }
 }
 
+// ------------------------------------------------- device-side repetition
+//
+// The tree of one repetition built without host round trips: the node list
+// of a level, its sampling plan, work items, split outcomes and the next
+// level's list all stay in device memory, so one tree level is a fixed
+// sequence of launches whose sizes come from device counters -- the body of
+// a CUDA-graph WHILE node that runs until no node is left to split.
+// Results equal the host-sequenced repetition's: the counter RNG is keyed by
+// node, nodes of a level are disjoint, and a node that fails (no seed pair,
+// an empty cluster or side) is retried with the next attempt index in the
+// next level instead of at once, which changes nothing but the order.
+
+constexpr uint32_t kPlanThreads = 1024;
+constexpr uint32_t kMaxSplitAttempts = 64;
+// Level iterations a repetition may take: far above any real tree (depth
+// <= 32, each node retried at most kMaxSplitAttempts times); past it the
+// loop stops and reports an error instead of running on.
+constexpr uint32_t kMaxLevelIterations = 8192;
+
+struct LevelCounts {
+    uint32_t cur, next, leaves, lloyd_items, part_items, iterations, restarts, fallbacks, nodes, leaf_work;
+    unsigned long long pairs;  // sum of b (b - 1) / 2 over the leaves
+};
+
+// Exclusive prefix sum of one value per thread over a CTA of kPlanThreads;
+// *total receives the sum.  Every thread calls it.
+__device__ __forceinline__ unsigned long long plan_scan(unsigned long long v, unsigned long long* __restrict__ wt,
+                                                        unsigned long long* total) {
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    unsigned long long incl = v;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == kWarp - 1) wt[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long t = wt[lane];
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, t, o);
+            if (lane >= o) t += y;
+        }
+        wt[lane] = t;
+    }
+    __syncthreads();
+    const unsigned long long base = warp > 0 ? wt[warp - 1] : 0ull;
+    *total = wt[kWarp - 1];
+    __syncthreads();
+    return base + incl - v;
+}
+
+// The level's sampling plan (rules of getSampleFromPercent / kmeansStartVecs,
+// as the host-sequenced level applies them; `table[n]` = sample count << 8 |
+// seed count): per node the CSR offsets of its draws, seeds and Lloyd list,
+// its Lloyd set (list or whole range) in the flag / id arrays, and its first
+// Lloyd work item.
+__global__ void __launch_bounds__(kPlanThreads)
+    k_level_plan(const uint32_t* __restrict__ start, const uint32_t* __restrict__ end, LevelCounts* __restrict__ cnt,
+                 const uint32_t* __restrict__ table, uint32_t small_threshold, uint64_t* __restrict__ draw_off,
+                 uint64_t* __restrict__ seed_off, uint64_t* __restrict__ lloyd_off, SeqNode* __restrict__ seq,
+                 uint64_t* __restrict__ lbegin, uint32_t* __restrict__ lfrom, uint32_t* __restrict__ item_off) {
+    __shared__ unsigned long long wt[kWarp];
+    const uint32_t count = cnt->cur;
+    const uint32_t per = (count + kPlanThreads - 1) / kPlanThreads;
+    const uint32_t b = threadIdx.x * per, e = min(count, b + per);
+    auto plan = [&](uint32_t i, uint32_t& draws, uint32_t& seeds, uint32_t& list, uint32_t& entries) {
+        const uint32_t n = end[i] - start[i];
+        const uint32_t packed = table[n];
+        const uint32_t S = packed & 0xFFu, samp = packed >> 8;
+        const bool large = n >= small_threshold;
+        draws = large ? samp : S;
+        seeds = min(draws, S);
+        list = large ? draws : 0u;
+        entries = list > 0 ? list : n;
+    };
+    unsigned long long sd = 0, ss = 0, sl = 0, sf = 0, si = 0;
+    for (uint32_t i = b; i < e; ++i) {
+        uint32_t draws, seeds, list, entries;
+        plan(i, draws, seeds, list, entries);
+        sd += draws;
+        ss += seeds;
+        sl += list;
+        sf += (entries + 15u) / 16u * 16u;
+        si += (entries + kChunk - 1) / kChunk;
+    }
+    unsigned long long td, ts, tl, tf, ti;
+    unsigned long long od = plan_scan(sd, wt, &td), os = plan_scan(ss, wt, &ts), ol = plan_scan(sl, wt, &tl);
+    unsigned long long of = plan_scan(sf, wt, &tf), oi = plan_scan(si, wt, &ti);
+    for (uint32_t i = b; i < e; ++i) {
+        uint32_t draws, seeds, list, entries;
+        plan(i, draws, seeds, list, entries);
+        draw_off[i] = od;
+        seed_off[i] = os;
+        lloyd_off[i] = ol;
+        seq[i] = {of, entries, 0u};
+        lbegin[i] = list > 0 ? ol : start[i];
+        lfrom[i] = list > 0 ? 1u : 0u;
+        item_off[i] = static_cast<uint32_t>(oi);
+        od += draws;
+        os += seeds;
+        ol += list;
+        of += (entries + 15u) / 16u * 16u;
+        oi += (entries + kChunk - 1) / kChunk;
+    }
+    if (threadIdx.x == 0) {
+        draw_off[count] = td;
+        seed_off[count] = ts;
+        lloyd_off[count] = tl;
+        item_off[count] = static_cast<uint32_t>(ti);
+        cnt->lloyd_items = static_cast<uint32_t>(ti);
+        cnt->nodes += count;
+    }
+}
+
+// Largest i in [0, count) with off[i] <= t (off non-decreasing, off[0] = 0).
+__device__ __forceinline__ uint32_t owner_of(const uint32_t* __restrict__ off, uint32_t count, uint32_t t) {
+    uint32_t lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Lloyd work items of the level (chunks of kChunk entries of a node's set).
+__global__ void k_lloyd_items(const LevelCounts* __restrict__ cnt, const uint32_t* __restrict__ item_off,
+                              const SeqNode* __restrict__ seq, const uint64_t* __restrict__ lbegin,
+                              const uint32_t* __restrict__ lfrom, Item* __restrict__ items) {
+    const uint32_t count = cnt->cur, total = cnt->lloyd_items;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t i = owner_of(item_off, count, t);
+        const uint64_t o = static_cast<uint64_t>(t - item_off[i]) * kChunk;
+        const uint64_t left = seq[i].len - o;
+        items[t] = {i | (lfrom[i] ? kListItem : 0u), static_cast<uint32_t>(left < kChunk ? left : kChunk),
+                    lbegin[i] + o, seq[i].fbase + o};
+    }
+}
+
+// Partition plan: the nodes that seeded and converged (ok) are cut into
+// kChunk-position items; ib / ie bound each node's items.
+__global__ void __launch_bounds__(kPlanThreads)
+    k_part_plan(const uint32_t* __restrict__ start, const uint32_t* __restrict__ end, LevelCounts* __restrict__ cnt,
+                const int32_t* __restrict__ ok, uint32_t* __restrict__ ib, uint32_t* __restrict__ ie) {
+    __shared__ unsigned long long wt[kWarp];
+    const uint32_t count = cnt->cur;
+    const uint32_t per = (count + kPlanThreads - 1) / kPlanThreads;
+    const uint32_t b = threadIdx.x * per, e = min(count, b + per);
+    unsigned long long si = 0;
+    for (uint32_t i = b; i < e; ++i) si += ok[i] ? (end[i] - start[i] + kChunk - 1) / kChunk : 0u;
+    unsigned long long ti;
+    unsigned long long oi = plan_scan(si, wt, &ti);
+    for (uint32_t i = b; i < e; ++i) {
+        ib[i] = static_cast<uint32_t>(oi);
+        oi += ok[i] ? (end[i] - start[i] + kChunk - 1) / kChunk : 0u;
+        ie[i] = static_cast<uint32_t>(oi);
+    }
+    if (threadIdx.x == 0) cnt->part_items = static_cast<uint32_t>(ti);
+}
+
+__global__ void k_part_items(const LevelCounts* __restrict__ cnt, const uint32_t* __restrict__ start,
+                             const uint32_t* __restrict__ end, const uint32_t* __restrict__ ib,
+                             Item* __restrict__ items) {
+    const uint32_t count = cnt->cur, total = cnt->part_items;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const uint32_t i = owner_of(ib, count, t);
+        const uint64_t o = static_cast<uint64_t>(start[i]) + static_cast<uint64_t>(t - ib[i]) * kChunk;
+        const uint64_t left = end[i] - o;
+        items[t] = {i, static_cast<uint32_t>(left < kChunk ? left : kChunk), o, o};
+    }
+}
+
+// Outcome of every node of the level: split at start + (side-true count), or
+// retried with the next attempt (no seed pair, an empty cluster or side), or
+// after kMaxSplitAttempts failures split at its index midpoint; children below
+// max_leaf points become leaves, the others the next level's nodes.
+__global__ void k_level_next(const uint32_t* __restrict__ start, const uint32_t* __restrict__ end,
+                             const uint32_t* __restrict__ base, const uint32_t* __restrict__ attempt,
+                             LevelCounts* __restrict__ cnt, const int32_t* __restrict__ ok,
+                             const uint32_t* __restrict__ node_true, const uint64_t* __restrict__ rep_params,
+                             uint32_t* __restrict__ nstart, uint32_t* __restrict__ nend, uint32_t* __restrict__ nbase,
+                             uint32_t* __restrict__ nattempt, uint32_t* __restrict__ leaf_start,
+                             uint32_t* __restrict__ leaf_end) {
+    const uint32_t count = cnt->cur;
+    const uint32_t max_leaf = static_cast<uint32_t>(rep_params[2]);
+    auto child = [&](uint32_t lo, uint32_t hi, uint32_t b) {
+        if (hi - lo < max_leaf) {
+            const uint32_t li = atomicAdd(&cnt->leaves, 1u);
+            leaf_start[li] = lo;
+            leaf_end[li] = hi;
+            const unsigned long long m = hi - lo;
+            atomicAdd(&cnt->pairs, m * (m - 1) / 2);
+        } else {
+            const uint32_t ni = atomicAdd(&cnt->next, 1u);
+            nstart[ni] = lo;
+            nend[ni] = hi;
+            nbase[ni] = b;
+            nattempt[ni] = 0;
+        }
+    };
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t s = start[i], e = end[i], b = base[i], a = attempt[i];
+        const uint32_t n = e - s, t = node_true[i];
+        uint32_t mid;
+        if (!ok[i] || t == 0 || t == n) {
+            atomicAdd(&cnt->restarts, 1u);
+            if (a + 1 < kMaxSplitAttempts) {
+                const uint32_t ni = atomicAdd(&cnt->next, 1u);
+                nstart[ni] = s;
+                nend[ni] = e;
+                nbase[ni] = b;
+                nattempt[ni] = a + 1;
+                continue;
+            }
+            atomicAdd(&cnt->fallbacks, 1u);
+            mid = s + n / 2;
+        } else {
+            mid = s + t;
+        }
+        child(s, mid, b);
+        child(mid, e, b);
+    }
+}
+
+// The next level becomes the current one; with `set_cond` the graph's WHILE
+// condition becomes (nodes left to split).
+__global__ void __launch_bounds__(kPlanThreads)
+    k_level_swap(LevelCounts* __restrict__ cnt, const uint32_t* __restrict__ nstart,
+                 const uint32_t* __restrict__ nend, const uint32_t* __restrict__ nbase,
+                 const uint32_t* __restrict__ nattempt, uint32_t* __restrict__ start, uint32_t* __restrict__ end,
+                 uint32_t* __restrict__ base, uint32_t* __restrict__ attempt, int32_t* __restrict__ error_flag,
+                 cudaGraphConditionalHandle cond, int set_cond) {
+    const bool runaway = cnt->iterations + 1 >= kMaxLevelIterations;
+    const uint32_t n = runaway ? 0u : cnt->next;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        start[i] = nstart[i];
+        end[i] = nend[i];
+        base[i] = nbase[i];
+        attempt[i] = nattempt[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (runaway) *error_flag = 1;
+        cnt->cur = n;
+        cnt->next = 0;
+        cnt->iterations += 1;
+        if (set_cond) cudaGraphSetConditional(cond, n > 0 ? 1u : 0u);
+    }
+}
+
+// Start of a repetition: indices 0..n-1 (done by k_iota), every point set's
+// root a node of the first level, or a leaf when it has fewer than max_leaf
+// points; counters cleared.
+__global__ void k_rep_init(const uint32_t* __restrict__ set_offsets, uint32_t nsets,
+                           const uint64_t* __restrict__ rep_params, LevelCounts* __restrict__ cnt,
+                           uint32_t* __restrict__ start, uint32_t* __restrict__ end, uint32_t* __restrict__ base,
+                           uint32_t* __restrict__ attempt, uint32_t* __restrict__ leaf_start,
+                           uint32_t* __restrict__ leaf_end, cudaGraphConditionalHandle cond, int set_cond) {
+    __shared__ uint32_t n_cur, n_leaf;
+    __shared__ unsigned long long pairs;
+    const uint32_t max_leaf = static_cast<uint32_t>(rep_params[2]);
+    if (threadIdx.x == 0) {
+        n_cur = 0;
+        n_leaf = 0;
+        pairs = 0;
+    }
+    __syncthreads();
+    for (uint32_t s = threadIdx.x; s < nsets; s += blockDim.x) {
+        const uint32_t lo = set_offsets[s], hi = set_offsets[s + 1];
+        if (hi - lo < max_leaf) {
+            const uint32_t li = atomicAdd(&n_leaf, 1u);
+            leaf_start[li] = lo;
+            leaf_end[li] = hi;
+            const unsigned long long m = hi - lo;
+            atomicAdd(&pairs, m * (m > 0 ? m - 1 : 0) / 2);
+        } else {
+            const uint32_t ni = atomicAdd(&n_cur, 1u);
+            start[ni] = lo;
+            end[ni] = hi;
+            base[ni] = lo;
+            attempt[ni] = 0;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *cnt = LevelCounts{};
+        cnt->cur = n_cur;
+        cnt->leaves = n_leaf;
+        cnt->pairs = pairs;
+        if (set_cond) cudaGraphSetConditional(cond, n_cur > 0 ? 1u : 0u);
+    }
+}
+
 }  // namespace
 
 void set_split_wait_limit(uint32_t polls) { KNNG_CUDA(cudaMemcpyToSymbol(tc::g_wait_limit, &polls, sizeof(polls))); }
@@ -700,6 +997,412 @@ void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, cons
     k_copy_back<<<ni, 256, 0, c.stream>>>(d_items, c.indices_tmp, c.indices, nullptr);
     c.launches += 5;
     KNNG_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------ host side
+
+// Buffers of the device-side repetition, sized for the context's points,
+// point sets and smallest bucket bound; the captured graphs (one per bucket
+// bound, Lloyd count and precision, and the pointers baked into them).
+struct DevRep {
+    uint32_t n = 0, nsets = 0, min_leaf = 0, small_threshold = 0, max_set = 0;
+    uint32_t node_cap = 0, lloyd_item_cap = 0, part_item_cap = 0, max_seed = 0;
+    uint64_t draw_cap = 0, entry_cap = 0;
+    std::vector<uint32_t> h_set_offsets;
+    std::vector<std::pair<void*, size_t>> allocs;
+    uint32_t *set_offsets, *table;
+    uint32_t *start, *end, *base, *attempt, *nstart, *nend, *nbase, *nattempt, *leaf_start, *leaf_end;
+    LevelCounts* cnt;
+    uint64_t* params;  // seed, repetition, max_leaf, 0
+    int32_t* error;    // [0] Lloyd sums, [1] BF16 bucket pass
+    uint64_t *draw_off, *seed_off, *lloyd_off;
+    uint32_t *seeds, *lloyd;
+    SeqNode* seq;
+    uint64_t* lbegin;
+    uint32_t *lfrom, *item_off, *lids, *litem_true;
+    Item* litems;
+    uint8_t* lflags;
+    uint32_t *first, *second;
+    int32_t* ok;
+    float *c1, *c2, *coefs, *offs;
+    uint32_t *ib, *ie, *item_true, *prefix, *node_true;
+    Item* pitems;
+    uint8_t* side_flags;
+    uint64_t* h_params = nullptr;  // pinned
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    struct Graph {
+        uint32_t max_leaf, lloyd_iters, precision;
+        const void* ptrs[8];
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+};
+
+namespace {
+
+// Packed sizing rules for every node size up to `max_n`: sample count << 8 |
+// seed count (the host's sample_count / start_count, so the device plan is
+// the host plan).  Computed once per process and grown on demand.
+std::mutex g_table_mutex;
+std::vector<uint32_t> g_count_table;
+
+const std::vector<uint32_t>& count_table(uint32_t max_n) {
+    std::lock_guard<std::mutex> lock(g_table_mutex);
+    const size_t have = g_count_table.size();
+    if (have > max_n) return g_count_table;
+    const size_t want = static_cast<size_t>(max_n) + 1;
+    g_count_table.resize(want);
+    const unsigned threads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    const size_t chunk = (want - have + threads - 1) / threads;
+    bool bad = false;
+    std::mutex bad_mutex;
+    for (unsigned t = 0; t < threads; ++t) {
+        const size_t lo = have + t * chunk, hi = std::min(want, lo + chunk);
+        if (lo >= hi) break;
+        pool.emplace_back([&, lo, hi] {
+            for (size_t m = lo; m < hi; ++m) {
+                const uint32_t v = static_cast<uint32_t>(m);
+                const uint32_t S = v >= 2 ? start_count(v) : 0u;
+                const uint32_t smp = v >= 2 ? sample_count(v) : 0u;
+                if (S > 0xFFu || smp > 0xFFFFFFu) {
+                    std::lock_guard<std::mutex> l(bad_mutex);
+                    bad = true;
+                }
+                g_count_table[m] = (smp << 8) | (S & 0xFFu);
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
+    if (bad) fail(KNNG_ERR_UNSUPPORTED, "point set too large for the device-side sampling plan");
+    return g_count_table;
+}
+
+template <class T>
+T* upload_into(Context& c, T* dst, const T* host, size_t count) {
+    if (count) KNNG_CUDA(cudaMemcpyAsync(dst, host, count * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+    return dst;
+}
+
+template <class T>
+T* rep_alloc(Context& c, DevRep& r, size_t count) {
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    void* p = dev_alloc(c, bytes);
+    r.allocs.emplace_back(p, bytes);
+    return static_cast<T*>(p);
+}
+
+void release_graphs(DevRep& r) {
+    for (auto& g : r.graphs) {
+        cudaGraphExecDestroy(g.exec);
+        cudaGraphDestroy(g.graph);
+    }
+    r.graphs.clear();
+}
+
+void release_buffers(Context& c, DevRep& r) {
+    release_graphs(r);
+    for (auto& a : r.allocs) dev_free(c, a.first, a.second);
+    r.allocs.clear();
+    r.n = 0;
+}
+
+// Buffers for the context's points and sets at bucket bound `max_leaf`.
+DevRep& ensure_devrep(Context& c, uint32_t max_leaf, uint32_t small_threshold) {
+    if (!c.devrep) {
+        c.devrep = new DevRep();
+        for (auto& e : c.devrep->ev) KNNG_CUDA(cudaEventCreate(&e));
+        void* p = nullptr;
+        KNNG_CUDA(cudaMallocHost(&p, 4 * sizeof(uint64_t)));
+        c.devrep->h_params = static_cast<uint64_t*>(p);
+    }
+    DevRep& r = *c.devrep;
+    const bool same = r.n == c.n && r.h_set_offsets == c.set_offsets && r.min_leaf <= max_leaf &&
+                      r.small_threshold == small_threshold;
+    if (same) return r;
+    KNNG_CUDA(cudaStreamSynchronize(c.stream));
+    release_buffers(c, r);
+    r.n = c.n;
+    r.h_set_offsets = c.set_offsets;
+    r.nsets = static_cast<uint32_t>(c.set_offsets.size() - 1);
+    r.min_leaf = max_leaf;
+    r.small_threshold = small_threshold;
+    r.max_set = 0;
+    for (uint32_t s = 0; s < r.nsets; ++s) r.max_set = std::max(r.max_set, c.set_offsets[s + 1] - c.set_offsets[s]);
+    const std::vector<uint32_t>& table = count_table(std::max(r.max_set, 2u));
+    // Capacities: a level's nodes hold >= max_leaf points each and are
+    // disjoint; draws are a large node's sample (at most r_max of its points)
+    // or a small node's seeds.
+    double r_max = 0.0;
+    for (uint32_t m = std::max(small_threshold, 2u); m <= r.max_set; ++m)
+        r_max = std::max(r_max, static_cast<double>(table[m] >> 8) / m);
+    r.max_seed = 1;
+    for (uint32_t m = 2; m <= r.max_set; ++m) r.max_seed = std::max(r.max_seed, table[m] & 0xFFu);
+    r.node_cap = r.n / std::max(max_leaf, 2u) + r.nsets + 1;
+    r.draw_cap = static_cast<uint64_t>(std::ceil(r_max * r.n)) + static_cast<uint64_t>(r.node_cap) * r.max_seed + 16;
+    r.entry_cap = r.n + r.draw_cap + 16ull * r.node_cap + 64;
+    r.lloyd_item_cap = static_cast<uint32_t>(r.entry_cap / kChunk) + r.node_cap + 1;
+    r.part_item_cap = r.n / kChunk + r.node_cap + 1;
+    const uint32_t nc = r.node_cap, ld = c.ld;
+    r.set_offsets = upload_into(c, rep_alloc<uint32_t>(c, r, r.nsets + 1), c.set_offsets.data(), r.nsets + 1);
+    r.table = upload_into(c, rep_alloc<uint32_t>(c, r, r.max_set + 1), table.data(), r.max_set + 1);
+    r.start = rep_alloc<uint32_t>(c, r, nc);
+    r.end = rep_alloc<uint32_t>(c, r, nc);
+    r.base = rep_alloc<uint32_t>(c, r, nc);
+    r.attempt = rep_alloc<uint32_t>(c, r, nc);
+    r.nstart = rep_alloc<uint32_t>(c, r, nc);
+    r.nend = rep_alloc<uint32_t>(c, r, nc);
+    r.nbase = rep_alloc<uint32_t>(c, r, nc);
+    r.nattempt = rep_alloc<uint32_t>(c, r, nc);
+    r.leaf_start = rep_alloc<uint32_t>(c, r, r.n + r.nsets);
+    r.leaf_end = rep_alloc<uint32_t>(c, r, r.n + r.nsets);
+    r.cnt = rep_alloc<LevelCounts>(c, r, 1);
+    r.params = rep_alloc<uint64_t>(c, r, 4);
+    r.error = rep_alloc<int32_t>(c, r, 4);
+    r.draw_off = rep_alloc<uint64_t>(c, r, nc + 1);
+    r.seed_off = rep_alloc<uint64_t>(c, r, nc + 1);
+    r.lloyd_off = rep_alloc<uint64_t>(c, r, nc + 1);
+    r.seeds = rep_alloc<uint32_t>(c, r, static_cast<size_t>(nc) * r.max_seed + 1);
+    r.lloyd = rep_alloc<uint32_t>(c, r, r.draw_cap);
+    r.seq = rep_alloc<SeqNode>(c, r, nc);
+    r.lbegin = rep_alloc<uint64_t>(c, r, nc);
+    r.lfrom = rep_alloc<uint32_t>(c, r, nc);
+    r.item_off = rep_alloc<uint32_t>(c, r, nc + 1);
+    r.litems = rep_alloc<Item>(c, r, r.lloyd_item_cap);
+    r.lflags = rep_alloc<uint8_t>(c, r, r.entry_cap);
+    r.lids = rep_alloc<uint32_t>(c, r, r.entry_cap);
+    r.litem_true = rep_alloc<uint32_t>(c, r, r.lloyd_item_cap + 1);
+    r.first = rep_alloc<uint32_t>(c, r, nc);
+    r.second = rep_alloc<uint32_t>(c, r, nc);
+    r.ok = rep_alloc<int32_t>(c, r, nc);
+    r.c1 = rep_alloc<float>(c, r, static_cast<size_t>(nc) * ld);
+    r.c2 = rep_alloc<float>(c, r, static_cast<size_t>(nc) * ld);
+    r.coefs = rep_alloc<float>(c, r, static_cast<size_t>(nc) * ld);
+    r.offs = rep_alloc<float>(c, r, nc);
+    r.ib = rep_alloc<uint32_t>(c, r, nc);
+    r.ie = rep_alloc<uint32_t>(c, r, nc);
+    r.pitems = rep_alloc<Item>(c, r, r.part_item_cap);
+    r.side_flags = rep_alloc<uint8_t>(c, r, static_cast<size_t>(r.n) + 16);
+    r.item_true = rep_alloc<uint32_t>(c, r, r.part_item_cap + 1);
+    r.prefix = rep_alloc<uint32_t>(c, r, r.part_item_cap + 1);
+    r.node_true = rep_alloc<uint32_t>(c, r, nc);
+    KNNG_CUDA(cudaStreamSynchronize(c.stream));
+    return r;
+}
+
+constexpr uint32_t kNodeGrid = 148 * 4;
+constexpr uint32_t kItemGrid = 148 * 8;
+constexpr uint32_t kThreadGrid = 148 * 2;
+
+// Start of a repetition: the error words cleared, indices 0..n-1, the sets'
+// roots as the first level.
+void enqueue_prologue(Context& c, DevRep& r, cudaGraphConditionalHandle cond, int set_cond) {
+    KNNG_CUDA(cudaMemsetAsync(r.error, 0, 4 * sizeof(int32_t), c.stream));
+    k_iota<<<std::min<uint32_t>((c.n + 255) / 256, 148 * 16), 256, 0, c.stream>>>(c.indices, c.n);
+    k_rep_init<<<1, 256, 0, c.stream>>>(r.set_offsets, r.nsets, r.params, r.cnt, r.start, r.end, r.base, r.attempt,
+                                        r.leaf_start, r.leaf_end, cond, set_cond);
+    c.launches += 2;
+    KNNG_CUDA(cudaGetLastError());
+}
+
+// One tree level: plan, draws, seeding, Lloyd iterations, partition, outcome.
+// Launch sizes do not depend on the level; no allocation, no host sync.
+void enqueue_level(Context& c, DevRep& r, uint32_t lloyd_iters, cudaGraphConditionalHandle cond, int set_cond) {
+    uint32_t* cur = &r.cnt->cur;
+    k_level_plan<<<1, kPlanThreads, 0, c.stream>>>(r.start, r.end, r.cnt, r.table, r.small_threshold, r.draw_off,
+                                                   r.seed_off, r.lloyd_off, r.seq, r.lbegin, r.lfrom, r.item_off);
+    k_draw_positions<<<kNodeGrid, 256, 0, c.stream>>>(r.start, r.end, r.base, r.attempt, r.draw_off, r.seed_off,
+                                                      r.lloyd_off, 0, 0, r.seeds, r.lloyd, cur, r.params);
+    k_lloyd_items<<<kThreadGrid, 256, 0, c.stream>>>(r.cnt, r.item_off, r.seq, r.lbegin, r.lfrom, r.litems);
+    KNNG_DISPATCH_D(c.d, {
+        const size_t fp_smem = static_cast<size_t>(r.max_seed) * c.ld * sizeof(float);
+        auto fp = k_farthest_pair<D>;
+        allow_max_smem(c, fp);
+        fp<<<kNodeGrid, kPairThreads, fp_smem, c.stream>>>(r.seed_off, r.seeds, c.indices, c.points, c.ld, r.first,
+                                                           r.second, r.ok, r.c1, r.c2, cur);
+        auto seqk = k_lloyd_seq<D>;
+        allow_max_smem(c, seqk);
+        for (uint32_t iter = 0; iter < lloyd_iters; ++iter) {
+            k_plane<D><<<kNodeGrid, 256, 0, c.stream>>>(r.c1, r.c2, c.ld, 0, r.coefs, r.offs, cur);
+            k_side<D><<<kItemGrid, kSideThreads, 0, c.stream>>>(r.litems, r.lloyd, c.indices, c.points, c.ld, r.coefs,
+                                                                r.offs, r.lflags, r.lids, r.litem_true,
+                                                                &r.cnt->lloyd_items);
+            seqk<<<kThreadGrid, kSeqThreads, seq_smem_bytes(D), c.stream>>>(r.seq, r.lflags, r.lids, c.points, c.ld,
+                                                                              r.c1, r.c2, r.ok, r.error, cur);
+        }
+        k_plane<D><<<kNodeGrid, 256, 0, c.stream>>>(r.c1, r.c2, c.ld, 0, r.coefs, r.offs, cur);
+        k_part_plan<<<1, kPlanThreads, 0, c.stream>>>(r.start, r.end, r.cnt, r.ok, r.ib, r.ie);
+        k_part_items<<<kThreadGrid, 256, 0, c.stream>>>(r.cnt, r.start, r.end, r.ib, r.pitems);
+        k_side<D><<<kItemGrid, kSideThreads, 0, c.stream>>>(r.pitems, nullptr, c.indices, c.points, c.ld, r.coefs,
+                                                            r.offs, r.side_flags, nullptr, r.item_true,
+                                                            &r.cnt->part_items);
+    });
+    k_scan_items<<<1, 1024, 0, c.stream>>>(r.item_true, 0, r.prefix, &r.cnt->part_items);
+    k_node_true<<<kThreadGrid, 256, 0, c.stream>>>(r.ib, r.ie, r.prefix, 0, r.node_true, cur);
+    k_scatter<<<kItemGrid, kSideThreads, 0, c.stream>>>(r.pitems, r.start, r.ib, r.node_true, r.prefix, r.side_flags,
+                                                        c.indices, c.indices_tmp, &r.cnt->part_items);
+    k_copy_back<<<kItemGrid, 256, 0, c.stream>>>(r.pitems, c.indices_tmp, c.indices, &r.cnt->part_items);
+    k_level_next<<<kThreadGrid, 256, 0, c.stream>>>(r.start, r.end, r.base, r.attempt, r.cnt, r.ok, r.node_true,
+                                                    r.params, r.nstart, r.nend, r.nbase, r.nattempt, r.leaf_start,
+                                                    r.leaf_end);
+    k_level_swap<<<1, kPlanThreads, 0, c.stream>>>(r.cnt, r.nstart, r.nend, r.nbase, r.nattempt, r.start, r.end,
+                                                   r.base, r.attempt, r.error + 2, cond, set_cond);
+    c.launches += 14 + 3 * lloyd_iters;
+    KNNG_CUDA(cudaGetLastError());
+}
+
+void enqueue_buckets(Context& c, DevRep& r, uint32_t max_leaf, uint32_t precision) {
+    if (precision == KNNG_PRECISION_BF16_RERANK)
+        launch_leaves_bf16_list(c, r.leaf_start, r.leaf_end, &r.cnt->leaves, &r.cnt->leaf_work,
+                                reinterpret_cast<uint32_t*>(r.error + 1));
+    else
+        launch_leaves_list(c, r.leaf_start, r.leaf_end, &r.cnt->leaves, &r.cnt->leaf_work, max_leaf - 1);
+}
+
+// The repetition as one graph: prologue, WHILE (nodes left) { level },
+// buckets, with timing events between the parts.
+DevRep::Graph& rep_graph(Context& c, DevRep& r, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t precision) {
+    const void* ptrs[8] = {c.points, c.indices, c.indices_tmp, c.set_dist, c.set_id, c.set_size, c.set_bound,
+                           reinterpret_cast<const void*>(static_cast<uintptr_t>(c.k))};
+    for (auto& g : r.graphs)
+        if (g.max_leaf == max_leaf && g.lloyd_iters == lloyd_iters && g.precision == precision &&
+            std::equal(ptrs, ptrs + 8, g.ptrs))
+            return g;
+    DevRep::Graph g{max_leaf, lloyd_iters, precision, {}, nullptr, nullptr};
+    std::copy(ptrs, ptrs + 8, g.ptrs);
+    const uint64_t launches0 = c.launches;
+    // Attributes first: nothing but stream work may happen during the capture.
+    KNNG_DISPATCH_D(c.d, {
+        allow_max_smem(c, k_farthest_pair<D>);
+        allow_max_smem(c, k_lloyd_seq<D>);
+    });
+    if (precision == KNNG_PRECISION_BF16_RERANK)
+        prepare_leaves_bf16_list(c);
+    else
+        prepare_leaves_list(c);
+    if (r.graphs.size() >= 4) {
+        KNNG_CUDA(cudaStreamSynchronize(c.stream));
+        release_graphs(r);
+    }
+    struct CaptureFlag {
+        Context& c;
+        explicit CaptureFlag(Context& cc) : c(cc) { c.capturing = true; }
+        ~CaptureFlag() { c.capturing = false; }
+    } capture_flag(c);
+    KNNG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    cudaGraphConditionalHandle cond{};
+    cudaGraph_t body = nullptr;
+    try {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t capg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        KNNG_CUDA(cudaStreamGetCaptureInfo(c.stream, &status, nullptr, &capg, &deps, &ndeps));
+        KNNG_CUDA(cudaGraphConditionalHandleCreate(&cond, capg, 0, cudaGraphCondAssignDefault));
+        KNNG_CUDA(cudaEventRecord(r.ev[0], c.stream));
+        enqueue_prologue(c, r, cond, 1);
+        KNNG_CUDA(cudaStreamGetCaptureInfo(c.stream, &status, nullptr, &capg, &deps, &ndeps));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        KNNG_CUDA(cudaGraphAddNode(&node, capg, deps, ndeps, &cp));
+        body = cp.conditional.phGraph_out[0];
+        KNNG_CUDA(cudaStreamUpdateCaptureDependencies(c.stream, &node, 1, cudaStreamSetCaptureDependencies));
+        KNNG_CUDA(cudaEventRecord(r.ev[1], c.stream));
+        enqueue_buckets(c, r, max_leaf, precision);
+        KNNG_CUDA(cudaEventRecord(r.ev[2], c.stream));
+    } catch (...) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(c.stream, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        cudaGetLastError();
+        throw;
+    }
+    KNNG_CUDA(cudaStreamEndCapture(c.stream, &g.graph));
+    // The WHILE node's body: one level, which sets the condition at its end.
+    KNNG_CUDA(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue_level(c, r, lloyd_iters, cond, 1);
+    } catch (...) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(c.stream, &junk);
+        cudaGraphDestroy(g.graph);
+        cudaGetLastError();
+        throw;
+    }
+    cudaGraph_t body_out = nullptr;
+    KNNG_CUDA(cudaStreamEndCapture(c.stream, &body_out));
+    KNNG_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    c.launches = launches0;  // capturing launched nothing
+    r.graphs.push_back(g);
+    return r.graphs.back();
+}
+
+}  // namespace
+
+void devrep_release(Context& c) {
+    if (!c.devrep) return;
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    release_buffers(c, *c.devrep);
+    for (auto& e : c.devrep->ev)
+        if (e) cudaEventDestroy(e);
+    if (c.devrep->h_params) cudaFreeHost(c.devrep->h_params);
+    delete c.devrep;
+    c.devrep = nullptr;
+}
+
+void run_rep_device(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold, uint64_t seed,
+                    uint32_t rep, uint32_t precision, bool graph, DevRepResult& out) {
+    DevRep& r = ensure_devrep(c, max_leaf, small_threshold);
+    r.h_params[0] = seed;
+    r.h_params[1] = rep;
+    r.h_params[2] = max_leaf;
+    r.h_params[3] = 0;
+    KNNG_CUDA(cudaMemcpyAsync(r.params, r.h_params, 4 * sizeof(uint64_t), cudaMemcpyHostToDevice, c.stream));
+    if (graph) {
+        DevRep::Graph& g = rep_graph(c, r, max_leaf, lloyd_iters, precision);
+        KNNG_CUDA(cudaGraphLaunch(g.exec, c.stream));
+    } else {
+        KNNG_CUDA(cudaEventRecord(r.ev[0], c.stream));
+        enqueue_prologue(c, r, cudaGraphConditionalHandle{}, 0);
+        for (uint32_t it = 0;; ++it) {
+            uint32_t cur = 0;
+            download(c, &cur, &r.cnt->cur, 1);
+            if (cur == 0) break;
+            if (it >= kMaxLevelIterations) fail(KNNG_ERR_CUDA, "tree levels: the level loop ran past its iteration limit");
+            enqueue_level(c, r, lloyd_iters, cudaGraphConditionalHandle{}, 0);
+        }
+        KNNG_CUDA(cudaEventRecord(r.ev[1], c.stream));
+        enqueue_buckets(c, r, max_leaf, precision);
+        KNNG_CUDA(cudaEventRecord(r.ev[2], c.stream));
+    }
+    LevelCounts h{};
+    download(c, &h, r.cnt, 1);
+    // Kernels the graph ran: prologue (2), every level, the bucket pass.
+    if (graph) c.launches += 3 + static_cast<uint64_t>(h.iterations) * (14 + 3 * lloyd_iters);
+    int32_t err[4] = {0, 0, 0, 0};
+    download(c, err, r.error, 4);
+    if (err[0]) fail(KNNG_ERR_CUDA, "Lloyd sums: a bulk-copy wait gave up");
+    if (err[1]) fail(KNNG_ERR_CUDA, "BF16 bucket pass: the MMA completion wait gave up");
+    if (err[2]) fail(KNNG_ERR_CUDA, "tree levels: the level loop ran past its iteration limit");
+    out.leaf_start.resize(h.leaves);
+    out.leaf_end.resize(h.leaves);
+    download(c, out.leaf_start.data(), r.leaf_start, h.leaves);
+    download(c, out.leaf_end.data(), r.leaf_end, h.leaves);
+    float ms = 0.f;
+    KNNG_CUDA(cudaEventElapsedTime(&ms, r.ev[0], r.ev[1]));
+    out.ms_split = ms;
+    KNNG_CUDA(cudaEventElapsedTime(&ms, r.ev[1], r.ev[2]));
+    out.ms_leaf = ms;
+    out.levels = h.iterations;
+    out.nodes = h.nodes;
+    out.restarts = h.restarts;
+    out.fallbacks = h.fallbacks;
+    out.pairs = h.pairs;
 }
 
 }  // namespace knng

@@ -415,3 +415,53 @@ def test_sets_snapshot_and_resume(knng_lib, tmp_path):
         b.refine()
         resumed = b.finalize()
     assert np.array_equal(resumed, straight)
+
+
+@pytest.mark.parametrize("loop", ["device", "host"])
+def test_rep_graph_equals_other_level_loops(knng_lib, monkeypatch, loop):
+    """A repetition run as one CUDA graph (device-side tree levels under a
+    WHILE node, then the persistent bucket pass over the device's leaf list)
+    leaves the same index permutation, leaves and sets, bit for bit, as the
+    same levels launched one by one and as the host-sequenced levels; over
+    several repetitions with alternating bucket bounds, a neighbour-of-
+    neighbour pass, and a batch of point sets."""
+    pts = workloads.gaussian_mixture(n=30_000, d=100, clusters=32, sigma=0.15, seed=21)
+
+    def run(mode):
+        if mode is None:
+            monkeypatch.delenv("KNNG_REP_LOOP", raising=False)
+        else:
+            monkeypatch.setenv("KNNG_REP_LOOP", mode)
+        out = []
+        with KnngContext(0) as c:
+            c.load_points(pts)
+            c.reset_sets(100)
+            for r, leaf in enumerate([257, 400, 257]):
+                c.run_rep(leaf, 2, 3000, seed=9, rep_index=r)
+                out.append((c.indices(), c.leaves(), c.sets()))
+            c.refine()
+            final = c.finalize(want_dists=True)
+        return out, final
+
+    graph, gfinal = run(None)
+    other, ofinal = run(loop)
+    for r, ((gi, gl, gs), (oi, ol, os_)) in enumerate(zip(graph, other)):
+        np.testing.assert_array_equal(gi, oi)
+        np.testing.assert_array_equal(gl[0], ol[0])
+        np.testing.assert_array_equal(gl[1], ol[1])
+        assert_sets_equal(gs, os_, f"rep {r}")
+    np.testing.assert_array_equal(gfinal[0], ofinal[0])
+    np.testing.assert_array_equal(gfinal[1].view(np.uint32), ofinal[1].view(np.uint32))
+    # A batch of sets of uneven size (one below the bucket bound).
+    sizes = [5000, 200, 12_000, 800]
+    sets = [workloads.gaussian_mixture(n=m, d=100, clusters=6, sigma=0.2, seed=60 + i) for i, m in enumerate(sizes)]
+    params = default_params(reps=2, refine=1, max_leaf=257, max_leaf_odd=400, lloyd_iters=2, seed=5)
+    monkeypatch.delenv("KNNG_REP_LOOP", raising=False)
+    with KnngContext(0) as c:
+        g_ids, g_d = c.build_batch(sets, params, want_dists=True)
+    monkeypatch.setenv("KNNG_REP_LOOP", loop)
+    with KnngContext(0) as c:
+        o_ids, o_d = c.build_batch(sets, params, want_dists=True)
+    for s in range(len(sets)):
+        np.testing.assert_array_equal(g_ids[s], o_ids[s])
+        np.testing.assert_array_equal(g_d[s].view(np.uint32), o_d[s].view(np.uint32))
