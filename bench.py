@@ -186,12 +186,10 @@ def dist_done(world: int):
 
 def workload_config(n: int, reps: int, refine: int, max_leaf: int, bf16: bool, world: int) -> dict:
     """The `config` object of the build line, the same for both arms."""
-    return {"workload": f"{n:,} x {DIM} f32, 1024-cluster Zipf(1.1) 24-d subspace mixture (seed {SEED}), "
-                        f"k={K}, leaf<={max_leaf - 1}, {reps} repetitions, {LLOYD_ITERS} Lloyd "
-                        f"iterations, {refine} neighbour-of-neighbour passes"
-                        + (", BF16 bucket estimates + FP32 re-rank" if bf16 else ", FP32"),
-            "n": n, "k": K, "reps": reps, "precision": "bf16_rerank" if bf16 else "fp32",
-            "parallelism": f"replicas x{world}", "l2": "input 4 GB > 126 MB L2; no flush between steps"}
+    return {"workload": f"{n:,} x {DIM} f32 1024-cluster Zipf(1.1) 24-d subspace mixture (seed {SEED}), "
+                        f"k={K}, leaf<={max_leaf - 1}, {reps} reps x {LLOYD_ITERS} Lloyd iters, {refine} top-up passes"
+                        + (", BF16 estimates + FP32 re-rank" if bf16 else ", FP32"),
+            "parallelism": f"replicas x{world}", "l2": "4 GB input > L2, no flush"}
 
 
 # ------------------------------------------------------------ reference arm
@@ -516,23 +514,36 @@ def batched_wave_points(sizes, wave_seed: int, device: str):
     return x.contiguous()
 
 
+def sig(x, digits: int = 4):
+    """x rounded to `digits` significant digits (keeps the bench line short)."""
+    if isinstance(x, float) and x != 0.0 and np.isfinite(x):
+        return float(f"{x:.{digits}g}")
+    return x
+
+
 def precision_summary(res: dict) -> dict:
-    """The precision object of the default line."""
+    """The precision object of the default line (the 100k-point config)."""
     f, b = res["fp32"], res["bf16_rerank"]
-    return {"workload": "100k config: 64 Gaussians, k=100, buckets<=256, 8 reps + 1 pass",
-            "fp32_ms": f["ms_per_build"], "bf16_rerank_ms": b["ms_per_build"], "speedup": res["speedup"],
-            "fp32_recall": f["recall"], "bf16_rerank_recall": b["recall"], "recall_change": res["recall_change"],
-            "dist_rel_err_max": b["dist_rel_err_max"], "dist_rel_err_mean": b["dist_rel_err_mean"],
-            "bf16_estimate_rel_err_max": res["bf16_estimate_rel_err_max"],
-            "bf16_estimate_rel_err_mean": res["bf16_estimate_rel_err_mean"]}
+    return {"fp32_ms": sig(f["ms_per_build"]), "bf16_ms": sig(b["ms_per_build"]), "speedup": sig(res["speedup"]),
+            "fp32_recall": sig(f["recall"]), "bf16_recall": sig(b["recall"]),
+            "dist_err_max": sig(b["dist_rel_err_max"], 2), "est_err_max": sig(res["bf16_estimate_rel_err_max"], 2),
+            "est_err_mean": sig(res["bf16_estimate_rel_err_mean"], 2)}
 
 
 def batched_summary(res: dict) -> dict:
-    """The batched object of the default line: the first wave of the batched config."""
-    return {"workload": "wave 1 of 5 of the batched config: " + str(res["sets"]) + " sets, 16-Gaussian mixtures, "
-                        "sizes log-uniform [1e3, 2e5], k=100, 4 reps + 2 passes",
-            "sets": res["sets"], "points": res["points"], "ms": res["ms"], "points_per_s": res["points_per_s"],
-            "min_recall": res["min_recall"], "mean_recall": res["mean_recall"]}
+    """The batched object of the default line: wave 1 of the batched config."""
+    return {"sets": res["sets"], "points": res["points"], "points_per_s": sig(res["points_per_s"]),
+            "min_recall": sig(res["min_recall"])}
+
+
+def serving_summary(res: dict) -> dict:
+    """The serving object of the default line."""
+    o, u = res["stream_50_per_s"], res["at_70pct_capacity"]
+    return {"at_50_per_s": {"p50_ms": sig(o["p50_ms"]), "p99_ms": sig(o["p99_ms"]), "pts_per_s": sig(o["points_per_s"]),
+                            "offered_over_capacity": sig(o["offered_over_capacity"], 3), "n": o["requests"]},
+            "at_70pct": {"rate": sig(u["rate_per_s"], 3), "p50_ms": sig(u["p50_ms"]), "p99_ms": sig(u["p99_ms"]),
+                         "pts_per_s": sig(u["points_per_s"]), "n": u["requests"]},
+            "recall_ok": bool(o["all_recall_ok"] and u["all_recall_ok"])}
 
 
 def run_batched(waves: int, device: int = 0) -> dict:
@@ -667,8 +678,8 @@ def run_ours(args):
             one()
             times.append(time.perf_counter() - t)
         e_ms = dist_max(1000.0 * statistics.mean(times), world)
-        e2e = {"value": world * n / (e_ms / 1000.0), "unit": "points/s", "h2d_bytes_per_step": n * DIM * 4,
-               "d2h_bytes_per_step": n * K * 4, "ms_per_step": e_ms}
+        e2e = {"value": sig(world * n / (e_ms / 1000.0)), "unit": "points/s", "h2d_bytes_per_step": n * DIM * 4,
+               "d2h_bytes_per_step": n * K * 4, "ms_per_step": sig(e_ms)}
 
     line = None
     if rank == 0:
@@ -691,12 +702,12 @@ def run_ours(args):
         # DRAM bytes of one launch from the committed ncu capture at 500k
         # points, scaled by the points processed.
         traffic = JOIN_DRAM_BYTES_500K * n / 500_000
-        roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": achieved / hbm_peak, "traffic": traffic,
+        roofline = {"bound": "hbm", "achieved": sig(achieved), "peak": hbm_peak, "unit": "GB/s",
+                    "frac": sig(achieved / hbm_peak), "traffic": sig(traffic),
                     "kernel": "k_join", "peak_source": "measured" if peaks else "fallback",
-                    "ms_per_launch": per_launch_ms, "share_of_step": join_ms / max(device_ms, 1e-9)}
+                    "ms_per_launch": sig(per_launch_ms), "share_of_step": sig(join_ms / max(device_ms, 1e-9), 3)}
         last = stats_list[-1]
-        stages = {k: round(last[v], 1) for k, v in (
+        stages = {k: round(last[v]) for k, v in (
             ("split", "ms_split"), ("buckets", "ms_leaf"), ("join", "ms_refine_join"), ("replay", "ms_refine_apply"),
             ("refine_prep", "ms_refine_prep"), ("finalize", "ms_finalize"))}
         line = {
@@ -704,7 +715,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(n, args.reps, args.refine, max_leaf, args.bf16, world),
-            "clocks": clock, "gpu_launches": launches, "roofline": roofline, "e2e": e2e,
+            "clocks": {k: clock[k] for k in ("sm_mhz", "sm_max_mhz", "reasons") if k in clock},
+            "gpu_launches": launches, "roofline": roofline, "e2e": e2e,
             "stages_ms_last_step": stages,
         }
     ctx.close()
@@ -714,7 +726,7 @@ def run_ours(args):
     if extras and args.extras:
         for key, fn in (("precision", lambda: precision_summary(run_precision(local, 3, cpu_reference=False))),
                         ("batched", lambda: batched_summary(run_batched(1, local))),
-                        ("serving", lambda: run_serving_pair(args.serving_requests, local))):
+                        ("serving", lambda: serving_summary(run_serving_pair(args.serving_requests, local)))):
             try:
                 line[key] = fn()
             except Exception as e:  # an extra figure must not hide the build number
@@ -724,10 +736,9 @@ def run_ours(args):
             res = reference_sample_rate(n, args.reps, args.refine, args.cpu_seconds, 1, 0)
             if res:
                 line["cpu_baseline"] = {
-                    "value": res["rates"][0], "unit": "points/s", "cores": res["cores"], "kind": "reference",
-                    "sample": f"the reference's splitKmeansBinaryProcess x{args.reps} then topUpSingle x{args.refine} "
-                              f"(std::thread-pool TBB stand-in, all host threads) on the first "
-                              f"{res['sample_points']:,} points of the same point set; points/s = sample / seconds"}
+                    "value": sig(res["rates"][0]), "unit": "points/s", "cores": res["cores"], "kind": "reference",
+                    "sample": f"reference splitKmeansBinaryProcess x{args.reps} + topUpSingle x{args.refine}, all host "
+                              f"threads, first {res['sample_points']:,} points of the same set"}
         except Exception as e:  # the baseline must not hide the GPU number
             line["cpu_baseline"] = {"error": str(e)[:200]}
     if rank == 0:
