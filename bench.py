@@ -681,6 +681,22 @@ def run_ours(args):
         e2e = {"value": sig(world * n / (e_ms / 1000.0)), "unit": "points/s", "h2d_bytes_per_step": n * DIM * 4,
                "d2h_bytes_per_step": n * K * 4, "ms_per_step": sig(e_ms)}
 
+    # Adaptive schedule on the same points: repetitions and passes until the
+    # recall estimated on 1,000 sampled points reaches 0.94 (at most 8 + 4);
+    # its recall is checked on the line's own 10k-point FP64 sample.
+    adaptive = None
+    if args.extras and not args.no_e2e and world == 1 and not args.bf16:
+        try:
+            ap = default_params(k=K, max_leaf=max_leaf, max_leaf_odd=0, lloyd_iters=LLOYD_ITERS, reps=8, refine=4,
+                                seed=SEED)
+            ast = Stats()
+            aids = ctx.build_adaptive(hin, 0.94, sample=1000, params=ap, stats=ast)
+            adaptive = {"target": 0.94, "reps": int(ast.reps_done), "passes": int(ast.refine_passes_done),
+                        "ms": sig(ast.ms_total + ast.ms_finalize), "recall_est": sig(ast.recall_estimate),
+                        "recall": sig(groundtruth.recall(aids.astype(np.int64), gt, q))}
+        except Exception as e:  # the adaptive figure must not hide the build number
+            adaptive = {"error": str(e)[:200]}
+
     line = None
     if rank == 0:
         peaks = {}
@@ -719,6 +735,8 @@ def run_ours(args):
             "gpu_launches": launches, "roofline": roofline, "e2e": e2e,
             "stages_ms_last_step": stages,
         }
+        if adaptive is not None:
+            line["adaptive"] = adaptive
     ctx.close()
     x = ids = None
     torch.cuda.empty_cache()

@@ -105,6 +105,8 @@ typedef struct knng_stats {
     uint64_t refine_join_launches; /* join-kernel launches */
     uint64_t refine_lost;     /* points redone by the per-point pass (pool region full) */
     uint64_t refine_passes_done; /* neighbour-of-neighbour passes run, whichever kernel ran them */
+    double recall_estimate;   /* knng_build_adaptive: recall on its sample at the end */
+    uint64_t estimate_queries;/* knng_build_adaptive: sampled points */
 } knng_stats;
 
 /* Fills the reference's parameters: k=100, max_leaf=200, max_leaf_odd=400,
@@ -128,6 +130,21 @@ const char* knng_last_error(const knng_context* ctx);
  * (optional, may be NULL); stats optional. */
 knng_status knng_build(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
                        const knng_params* params, uint32_t* out_ids, float* out_dists, knng_stats* stats);
+
+/* Adaptive schedule, for a recall target instead of fixed counts or a time
+ * budget (the reference repeats until a wall-clock bound, then tops up:
+ * SolutionKmeans::constructResult, src/SolutionKmeans.hpp:579-604).  The
+ * exact k nearest of `sample` evenly spaced points are found on the device
+ * once (FP32 distances in the reference's order); after the first
+ * min(2, params->reps) repetitions, neighbour-of-neighbour passes and further
+ * repetitions are added -- a pass after each repetition, a second pass while
+ * the target is missed, then another repetition -- until the recall
+ * estimated on the sample reaches target_recall or params->reps repetitions
+ * (0: up to 64) and params->refine passes have run.  stats->reps_done,
+ * refine_passes_done and recall_estimate report what ran and reached. */
+knng_status knng_build_adaptive(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                                const knng_params* params, double target_recall, uint32_t sample, uint32_t* out_ids,
+                                float* out_dists, knng_stats* stats);
 
 /* The same with device-resident input and output (pointers into the
  * context's device memory space); synchronous. */

@@ -37,7 +37,7 @@ EXPORTED = [
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
     "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_debug_set_wait_limit", "knng_refine_pointwise_noalloc",
     "knng_build_batch",
-    "knng_build_timed", "knng_save_sets", "knng_load_sets", "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
+    "knng_build_timed", "knng_build_adaptive", "knng_save_sets", "knng_load_sets", "knng_job_reservation", "knng_server_create", "knng_server_submit", "knng_server_poll", "knng_server_wait",
     "knng_server_job_error", "knng_server_release", "knng_server_destroy",
 ]
 
@@ -62,7 +62,7 @@ class Stats(Structure):
         ("refine_pairs", c_uint64), ("refine_filter_pass", c_uint64), ("refine_member_skip", c_uint64),
         ("refine_exact", c_uint64), ("refine_emits", c_uint64), ("refine_overflow", c_uint64),
         ("ms_refine_prep", c_double), ("refine_join_launches", c_uint64), ("refine_lost", c_uint64),
-        ("refine_passes_done", c_uint64),
+        ("refine_passes_done", c_uint64), ("recall_estimate", c_double), ("estimate_queries", c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -126,6 +126,8 @@ def load_library(path: str = LIB_PATH):
         "knng_load_sets": (c_int, [P, c_char_p]),
         "knng_build_timed": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), c_uint64, c_uint64, P, P,
                                      POINTER(Stats)]),
+        "knng_build_adaptive": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), c_double, c_uint32, P, P,
+                                        POINTER(Stats)]),
         "knng_build_batch": (c_int, [P, P, c_uint32, c_uint32, c_uint64, P, c_uint32, c_int, POINTER(Params), P, P,
                                      POINTER(Stats)]),
         "knng_job_reservation": (c_uint64, [c_uint32, c_uint32, c_uint32]),
@@ -240,6 +242,22 @@ class KnngContext:
         st = stats if stats is not None else Stats()
         self._check(self._lib.knng_build_timed(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p), build_ms,
                                                refine_ms, _ptr(ids), _ptr(dists), ctypes.byref(st)))
+        self.n, self.d, self.k = n, d, p.k
+        return (ids, dists) if want_dists else ids
+
+    def build_adaptive(self, points: np.ndarray, target_recall: float, sample: int = 1000,
+                       params: Params | None = None, want_dists: bool = False, stats: Stats | None = None):
+        """knng_build_adaptive: repetitions and passes until the recall estimated
+        on `sample` points reaches target_recall (params.reps / params.refine
+        are the maxima)."""
+        pts = _f32(points)
+        n, d = pts.shape
+        p = params or default_params()
+        ids = np.empty((n, p.k), np.uint32)
+        dists = np.empty((n, p.k), np.float32) if want_dists else None
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_build_adaptive(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p),
+                                                  target_recall, sample, _ptr(ids), _ptr(dists), ctypes.byref(st)))
         self.n, self.d, self.k = n, d, p.k
         return (ids, dists) if want_dists else ids
 

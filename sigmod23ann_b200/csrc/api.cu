@@ -564,6 +564,65 @@ void build_all(Context& c, const knng_params* p, knng_stats* stats, uint64_t bui
     }
 }
 
+// Adaptive schedule: repetitions and neighbour-of-neighbour passes until the
+// recall estimated on `sample` evenly spaced points (their exact k nearest
+// found on the device once) reaches `target`.  After the first
+// min(2, max reps) repetitions: a pass follows every repetition, a second
+// pass follows if the target is still missed, then another repetition; at
+// most p->reps repetitions (0: 64) and p->refine passes.  The recall is
+// estimated after every step.
+void build_adaptive(Context& c, const knng_params* p, double target, uint32_t sample, knng_stats* stats) {
+    alloc_sets(c, p->k);
+    EventPair total_t(c);
+    const uint64_t launches0 = c.launches;
+    const uint32_t q = std::max<uint32_t>(1, std::min(sample, c.n));
+    std::vector<uint32_t> hq(q);
+    for (uint32_t i = 0; i < q; ++i) hq[i] = static_cast<uint32_t>((static_cast<uint64_t>(i) * c.n) / q);
+    uint32_t* d_q = upload(c, "adaptive_queries", hq.data(), q);
+    auto* d_truth = static_cast<uint32_t*>(scratch(c, "adaptive_truth", static_cast<size_t>(q) * c.k * sizeof(uint32_t)));
+    sample_knn(c, d_q, q, d_truth);
+    const uint32_t max_reps = p->reps ? p->reps : 64u, max_passes = p->refine;
+    const uint32_t min_reps = std::min(2u, max_reps);
+    uint32_t reps = 0, passes = 0, passes_since_rep = 0;
+    double est = 0.0;
+    auto rep_step = [&] {
+        const uint32_t leaf = (p->max_leaf_odd != 0 && (reps % 2 == 1)) ? p->max_leaf_odd : p->max_leaf;
+        RepStats st;
+        run_rep(c, leaf, p->lloyd_iters, p->small_threshold, p->seed, reps, st, stats, p->precision);
+        add_rep_stats(stats, st);
+        if (stats) stats->reps_done += 1;
+        ++reps;
+        passes_since_rep = 0;
+    };
+    auto pass_step = [&] {
+        EventPair rt(c);
+        const uint64_t ch = run_refine(c);
+        add_refine_stats(stats, c, ch, rt.stop(c));
+        ++passes;
+        ++passes_since_rep;
+    };
+    while (reps < min_reps) rep_step();
+    est = sample_recall(c, d_q, q, d_truth);
+    while (est < target) {
+        if (passes_since_rep < 2 && passes < max_passes)
+            pass_step();
+        else if (reps < max_reps)
+            rep_step();
+        else if (passes < max_passes)
+            pass_step();
+        else
+            break;
+        est = sample_recall(c, d_q, q, d_truth);
+    }
+    const double ms = total_t.stop(c);
+    if (stats) {
+        stats->ms_total += ms;
+        stats->kernel_launches += c.launches - launches0;
+        stats->recall_estimate = est;
+        stats->estimate_queries = q;
+    }
+}
+
 template <class F>
 knng_status guarded(knng_context* ctx, F&& f) {
     Context* c = reinterpret_cast<Context*>(ctx);
@@ -1011,6 +1070,28 @@ knng_status knng_build_timed(knng_context* ctx, const float* points, uint32_t n,
         if (stats) std::memset(stats, 0, sizeof(*stats));
         knng::load_points(c, points, n, d, ld_bytes, false, false);
         knng::build_all(c, params, stats, build_ms, refine_ms);
+        const size_t nk = static_cast<size_t>(c.n) * c.k;
+        knng::EventPair ft(c);
+        uint32_t* d_ids = static_cast<uint32_t*>(knng::scratch(c, "fin_ids", nk * sizeof(uint32_t)));
+        float* d_dist = out_dists ? static_cast<float*>(knng::scratch(c, "fin_dist", nk * sizeof(float))) : nullptr;
+        knng::launch_finalize(c, d_ids, d_dist);
+        if (stats) stats->ms_finalize += ft.stop(c);
+        knng::download(c, out_ids, d_ids, nk);
+        if (out_dists) knng::download(c, out_dists, d_dist, nk);
+    });
+}
+
+knng_status knng_build_adaptive(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                                const knng_params* params, double target_recall, uint32_t sample, uint32_t* out_ids,
+                                float* out_dists, knng_stats* stats) {
+    return knng::guarded(ctx, [&](Context& c) {
+        knng::validate_params(params);
+        if (!out_ids) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null output");
+        if (!(target_recall > 0.0 && target_recall <= 1.0)) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "target recall must be in (0, 1]");
+        if (sample == 0) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "sample must be positive");
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        knng::load_points(c, points, n, d, ld_bytes, false, false);
+        knng::build_adaptive(c, params, target_recall, sample, stats);
         const size_t nk = static_cast<size_t>(c.n) * c.k;
         knng::EventPair ft(c);
         uint32_t* d_ids = static_cast<uint32_t*>(knng::scratch(c, "fin_ids", nk * sizeof(uint32_t)));

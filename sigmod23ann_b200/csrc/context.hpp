@@ -223,6 +223,11 @@ void launch_leaves_list(Context& c, const uint32_t* d_starts, const uint32_t* d_
                         uint32_t* d_work, uint32_t max_bucket);
 void launch_leaves_bf16_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
                              uint32_t* d_work, uint32_t* d_error);
+// Exact k nearest points (FP32 distances in the reference's order) of the
+// nq points d_queries, ids into d_truth (nq x k, kNone past the end).
+void sample_knn(Context& c, const uint32_t* d_queries, uint32_t nq, uint32_t* d_truth);
+// Mean fraction of each sampled point's true k nearest held by its set.
+double sample_recall(Context& c, const uint32_t* d_queries, uint32_t nq, const uint32_t* d_truth);
 // Kernel attributes of the two list launchers, set before a graph capture.
 void prepare_leaves_list(Context& c);
 void prepare_leaves_bf16_list(Context& c);

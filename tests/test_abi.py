@@ -50,7 +50,7 @@ def test_struct_layouts_match_header(tmp_path):
     import subprocess
 
     assert ctypes.sizeof(api.Params) == 40
-    assert ctypes.sizeof(api.Stats) == 10 * 8 + 20 * 8
+    assert ctypes.sizeof(api.Stats) == 11 * 8 + 21 * 8
     checks = [("knng_stats", name) for name, _ in api.Stats._fields_] + \
              [("knng_params", name) for name, _ in api.Params._fields_]
     src = tmp_path / "layout.c"
