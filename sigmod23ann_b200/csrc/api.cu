@@ -36,10 +36,10 @@ void fail(knng_status s, const std::string& msg) { throw Error{s, msg}; }
 
 void check_cuda(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;
-    if (e == cudaErrorMemoryAllocation) {
-        cudaGetLastError();
-        fail(KNNG_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
-    }
+    // A non-sticky error stays as the thread's last error until read; clear
+    // it so the next call on this context does not report it again.
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation) fail(KNNG_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
     fail(KNNG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 

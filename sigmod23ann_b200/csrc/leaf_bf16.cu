@@ -180,11 +180,16 @@ __global__ void __launch_bounds__(kBfThreads, 1)
     __syncthreads();
     for (int k = tid; k < D; k += kBfThreads) centre[k] = pts[static_cast<size_t>(ids[0]) * ld + k];
     __syncthreads();
-    for (uint32_t t = tid; t < b; t += kBfThreads) norms[t] = centred_norm<D>(pts, ld, ids[t], centre);
+    // Buckets of at most 129 points keep every other member: no estimates,
+    // and the tiles' space holds only the kept positions.
     const bool keep_all = b - 1 <= static_cast<uint32_t>(kKeep);
+    if (!keep_all)
+        for (uint32_t t = tid; t < b; t += kBfThreads) norms[t] = centred_norm<D>(pts, ld, ids[t], centre);
     for (uint32_t rb = 0; rb < b && healthy; rb += kBfRows) {
         const uint32_t cnt = min(static_cast<uint32_t>(kBfRows), b - rb);
-        stage_bf16<D>(A, ids + rb, cnt, pts, ld, centre);
+        // The A tile overlays `keep`: staged only when estimates are made,
+        // and read (by the MMA) only behind the column loop's barriers.
+        if (!keep_all) stage_bf16<D>(A, ids + rb, cnt, pts, ld, centre);
         // Selection state of the row this thread owns (warps 0-3: TMEM lane r).
         const uint32_t r = static_cast<uint32_t>(warp * kWarp + lane);
         const uint32_t i = rb + r;  // bucket position of the row's point

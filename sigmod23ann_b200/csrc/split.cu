@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <limits>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -1300,7 +1301,7 @@ DevRep::Graph& rep_graph(Context& c, DevRep& r, uint32_t max_leaf, uint32_t lloy
         size_t ndeps = 0;
         KNNG_CUDA(cudaStreamGetCaptureInfo(c.stream, &status, nullptr, &capg, &deps, &ndeps));
         KNNG_CUDA(cudaGraphConditionalHandleCreate(&cond, capg, 0, cudaGraphCondAssignDefault));
-        KNNG_CUDA(cudaEventRecord(r.ev[0], c.stream));
+        KNNG_CUDA(cudaEventRecordWithFlags(r.ev[0], c.stream, cudaEventRecordExternal));
         enqueue_prologue(c, r, cond, 1);
         KNNG_CUDA(cudaStreamGetCaptureInfo(c.stream, &status, nullptr, &capg, &deps, &ndeps));
         cudaGraphNodeParams cp{};
@@ -1312,9 +1313,9 @@ DevRep::Graph& rep_graph(Context& c, DevRep& r, uint32_t max_leaf, uint32_t lloy
         KNNG_CUDA(cudaGraphAddNode(&node, capg, deps, ndeps, &cp));
         body = cp.conditional.phGraph_out[0];
         KNNG_CUDA(cudaStreamUpdateCaptureDependencies(c.stream, &node, 1, cudaStreamSetCaptureDependencies));
-        KNNG_CUDA(cudaEventRecord(r.ev[1], c.stream));
+        KNNG_CUDA(cudaEventRecordWithFlags(r.ev[1], c.stream, cudaEventRecordExternal));
         enqueue_buckets(c, r, max_leaf, precision);
-        KNNG_CUDA(cudaEventRecord(r.ev[2], c.stream));
+        KNNG_CUDA(cudaEventRecordWithFlags(r.ev[2], c.stream, cudaEventRecordExternal));
     } catch (...) {
         cudaGraph_t junk = nullptr;
         cudaStreamEndCapture(c.stream, &junk);
@@ -1343,6 +1344,17 @@ DevRep::Graph& rep_graph(Context& c, DevRep& r, uint32_t max_leaf, uint32_t lloy
 }
 
 }  // namespace
+
+// Device time between two recorded events; NaN when the runtime cannot
+// report it (the timings are diagnostics, the build's result stands).
+static float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        return std::numeric_limits<float>::quiet_NaN();
+    }
+    return ms;
+}
 
 void devrep_release(Context& c) {
     if (!c.devrep) return;
@@ -1393,11 +1405,8 @@ void run_rep_device(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_
     out.leaf_end.resize(h.leaves);
     download(c, out.leaf_start.data(), r.leaf_start, h.leaves);
     download(c, out.leaf_end.data(), r.leaf_end, h.leaves);
-    float ms = 0.f;
-    KNNG_CUDA(cudaEventElapsedTime(&ms, r.ev[0], r.ev[1]));
-    out.ms_split = ms;
-    KNNG_CUDA(cudaEventElapsedTime(&ms, r.ev[1], r.ev[2]));
-    out.ms_leaf = ms;
+    out.ms_split = elapsed_ms(r.ev[0], r.ev[1]);
+    out.ms_leaf = elapsed_ms(r.ev[1], r.ev[2]);
     out.levels = h.iterations;
     out.nodes = h.nodes;
     out.restarts = h.restarts;
