@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <mutex>
 #include <vector>
 
@@ -300,10 +301,11 @@ __global__ void k_rev_fill(const uint32_t* __restrict__ snap, uint32_t n, int K,
     }
 }
 
-constexpr int kJoinThreads = 512;
-constexpr int kJoinWarps = kJoinThreads / kWarp;  // 16
+constexpr int kJoinThreads = 256;
+constexpr int kJoinWarps = kJoinThreads / kWarp;  // 8
+constexpr int kJoinPerSm = 2;                     // CTAs per SM: one's waits overlap the other's work
 constexpr int kTile = 128;                        // MMA M: rows of R(q) per chunk
-constexpr int kGroupCols = 32;                    // columns one thread filters (4 groups of 32)
+constexpr int kGroupCols = 64;                    // columns one thread filters (2 groups of 64)
 
 // FP16 operand tiles, chunk-major: K padded to the MMA step of 16, a row held
 // as KP / 8 chunks of 16 bytes (8 halves).
@@ -322,13 +324,14 @@ __host__ __device__ constexpr uint32_t join_cols(uint32_t K) { return K <= 16 ? 
 // rows spread over the banks).
 __host__ __device__ constexpr uint32_t list_stride(uint32_t K) { return (K & 3u) == 0 ? K : (K | 1u); }
 
-// Dynamic shared memory of k_join (byte offsets).  rows_a / rows_b: the
-// original FP32 rows of R(q) (a chunk of up to 128) and of S(q), row-major;
-// they feed both the centred FP16 tiles and the exact distances.  tiles: the
-// A' and B' operand tiles, and once the MMA has read them the lists S(p) of
-// the chunk's rows.  x: per-thread pair masks, member masks, prefix sums.
+// Dynamic shared memory of k_join (byte offsets).  rows_b: the original FP32
+// rows of S(q), row-major, bulk-copied once per q; they feed the centred B'
+// tile and the column side of the exact distances (the rows of R(q) are read
+// from global memory, so that two CTAs fit an SM).  tiles: the A' and B'
+// operand tiles, and once the MMA has read them the lists S(p) of the chunk's
+// rows.  x: per-thread pair masks, member masks, prefix sums.
 struct JoinSmem {
-    uint32_t rows_a, rows_b, tiles, tile_b, norm_a, norm_b, rt_a, rt_b, bnd, pid, cid, fullrow, centre, x, bytes;
+    uint32_t rows_b, tiles, tile_b, norm_a, norm_b, rt_a, rt_b, bnd, pid, cid, fullrow, centre, x, bytes;
 };
 
 __host__ __device__ inline JoinSmem join_smem(int D, uint32_t K) {
@@ -337,8 +340,7 @@ __host__ __device__ inline JoinSmem join_smem(int D, uint32_t K) {
     const uint32_t tiles_bytes = (kTile + NB) * KP * 2;
     const uint32_t lists_bytes = kTile * list_stride(K) * 4;
     JoinSmem s{};
-    s.rows_a = 0;
-    s.rows_b = s.rows_a + kTile * static_cast<uint32_t>(D) * 4;
+    s.rows_b = 0;
     s.tiles = (s.rows_b + NB * static_cast<uint32_t>(D) * 4 + 127) / 128 * 128;
     s.tile_b = s.tiles + kTile * KP * 2;
     s.norm_a = s.tiles + ((tiles_bytes > lists_bytes ? tiles_bytes : lists_bytes) + 15) / 16 * 16;
@@ -434,16 +436,19 @@ __device__ __forceinline__ void pair_next(PairCursor& c, const unsigned long lon
 __device__ __forceinline__ int pair_row(int o) { return ((o / kWarp) % 4) * kWarp + (o % kWarp); }
 __device__ __forceinline__ int pair_col(int o, int bit) { return ((o / kWarp) / 4) * kGroupCols + bit; }
 
-// Centred FP16 operand rows from FP32 rows in shared memory.  Two threads
-// per row (t = 2r + h; half h converts chunks [h*HALF, (h+1)*HALF)): row r
-// (r < count, else zeros) minus `centre`, rounded to FP16, into a
-// chunk-major tile of `R` rows (chunk c of row r at c*R*16 + r*16).  Writes
-// the row's squared norm (FP32, of the centred FP32 values; both halves
-// summed in a fixed order) and its absolute error term 2^-19 |x'| (+inf when
-// a value does not fit FP16's range, so that the filter keeps every pair of
-// the row).  All 32 lanes of a warp call it; t below 2R do work.
-template <int D>
-__device__ __forceinline__ void convert_rows(const float* __restrict__ rows, uint32_t count, uint32_t R,
+// Centred FP16 operand rows.  Two threads per row (t = 2r + h; half h
+// converts chunks [h*HALF, (h+1)*HALF)): row r (r < count, else zeros) minus
+// `centre`, rounded to FP16, into a chunk-major tile of `R` rows (chunk c of
+// row r at c*R*16 + r*16).  The FP32 source row r is rows + r * stride, or
+// with kGather rows + ids[r] * stride in global memory (read through the
+// read-only path, every load of the thread in flight at once).  Writes the
+// row's squared norm (FP32, of the centred FP32 values; both halves summed in
+// a fixed order) and its absolute error term 2^-19 |x'| (+inf when a value
+// does not fit FP16's range, so that the filter keeps every pair of the row).
+// All 32 lanes of a warp call it; t below 2R do work.
+template <int D, bool kGather>
+__device__ __forceinline__ void convert_rows(const float* __restrict__ rows, const uint32_t* __restrict__ ids,
+                                             size_t stride, uint32_t count, uint32_t R,
                                              unsigned char* __restrict__ tile, const float* __restrict__ centre,
                                              float* __restrict__ norm, float* __restrict__ rt, int t) {
     constexpr int CH = JoinLayout<D>::CH;
@@ -453,7 +458,17 @@ __device__ __forceinline__ void convert_rows(const float* __restrict__ rows, uin
     float s = 0.0f, mx = 0.0f;
     if (r < R) {
         const bool live = r < count;
-#pragma unroll 1
+        const float* row = rows + (live ? (kGather ? static_cast<size_t>(ids[r]) : r) * stride : 0);
+        float4 a[2 * HALF];
+#pragma unroll
+        for (int i = 0; i < 2 * HALF; ++i) {
+            const int k = 8 * (h * HALF + i / 2) + 4 * (i % 2);
+            a[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (live && h * HALF + i / 2 < CH && k < D)
+                a[i] = kGather ? __ldg(reinterpret_cast<const float4*>(row + k))
+                               : *reinterpret_cast<const float4*>(row + k);
+        }
+#pragma unroll
         for (int i = 0; i < HALF; ++i) {
             const int c = h * HALF + i;
             if (c >= CH) break;
@@ -463,9 +478,10 @@ __device__ __forceinline__ void convert_rows(const float* __restrict__ rows, uin
                 const int k = 8 * c + 4 * q;
                 float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (live && k < D) {
-                    const float4 a = *reinterpret_cast<const float4*>(rows + static_cast<size_t>(r) * D + k);
                     const float4 m = *reinterpret_cast<const float4*>(centre + k);
-                    x = make_float4(__fsub_rn(a.x, m.x), __fsub_rn(a.y, m.y), __fsub_rn(a.z, m.z), __fsub_rn(a.w, m.w));
+                    const float4 v4 = a[2 * i + q];
+                    x = make_float4(__fsub_rn(v4.x, m.x), __fsub_rn(v4.y, m.y), __fsub_rn(v4.z, m.z),
+                                    __fsub_rn(v4.w, m.w));
                 }
                 v[4 * q + 0] = x.x;
                 v[4 * q + 1] = x.y;
@@ -496,6 +512,21 @@ __device__ __forceinline__ void convert_rows(const float* __restrict__ rows, uin
     }
 }
 
+// Phase clocks of k_join (built with -DKNNG_JOIN_PHASES only): thread 0 of
+// each CTA adds the clock64 time between consecutive marks to phase slot i;
+// the sums land in counters[8 + i].
+#ifdef KNNG_JOIN_PHASES
+constexpr int kJoinPhases = 12;
+#define JOIN_MARK(i)                     \
+    if (tid == 0) {                      \
+        const long long t1_ = clock64(); \
+        ph_[i] += t1_ - t0_;             \
+        t0_ = t1_;                       \
+    }
+#else
+#define JOIN_MARK(i)
+#endif
+
 // The local join of one neighbour-of-neighbour pass.  For every point q (taken
 // in `order`, the last repetition's leaf order, through the work counter):
 // the rows R(q) (points whose snapshot list holds q), in chunks of 128,
@@ -520,7 +551,7 @@ __device__ __forceinline__ void convert_rows(const float* __restrict__ rows, uin
 // the region is full the record is dropped and lost[p] set; the CTA's final
 // pool fill is written to pool_fill[blockIdx.x].
 template <int D>
-__global__ void __launch_bounds__(kJoinThreads, 1)
+__global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
     k_join(const uint32_t* __restrict__ snap, const unsigned long long* __restrict__ rev_off,
            const uint32_t* __restrict__ rev, const float* __restrict__ pts, int ld, const float* __restrict__ bound,
            const uint32_t* __restrict__ set_size, int K, uint32_t n, uint32_t slots,
@@ -532,7 +563,6 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     extern __shared__ __align__(1024) unsigned char smem[];
     const JoinSmem S = join_smem(D, static_cast<uint32_t>(K));
     const uint32_t NB = join_cols(static_cast<uint32_t>(K));
-    float* rows_a = reinterpret_cast<float*>(smem + S.rows_a);
     float* rows_b = reinterpret_cast<float*>(smem + S.rows_b);
     unsigned char* tile_a = smem + S.tiles;
     unsigned char* tile_b = smem + S.tile_b;
@@ -578,6 +608,10 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     const int quarter = warp % 4, group = warp / 4;
     const int row = quarter * kWarp + lane;  // TMEM lane / tile row this thread filters
     const unsigned lt = (1u << lane) - 1u;
+#ifdef KNNG_JOIN_PHASES
+    long long ph_[kJoinPhases] = {};
+    long long t0_ = clock64();
+#endif
     int search_top = 1;  // largest power of two <= K (branch-free lower bound)
     while (search_top * 2 <= K) search_top *= 2;
     // Waits on this CTA's own copies and MMAs; a wait that gives up marks the
@@ -596,6 +630,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
         if (tid == 0) work_s[it & 1u] = atomicAdd(work, 1u);
         __syncthreads();
         const uint32_t w = work_s[it & 1u];
+        JOIN_MARK(0)
         if (w >= n) break;
         const uint32_t q = order ? order[w] : w;
         const unsigned long long rb = rev_off[q], re = rev_off[q + 1];
@@ -626,6 +661,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
         }
         for (int j = tid; j < D; j += kJoinThreads) centre[j] = pts[static_cast<size_t>(q) * ld + j];
         __syncthreads();
+        JOIN_MARK(1)
         const uint32_t nc = ncols_s;
         for (unsigned long long cb = rb; cb < re && healthy; cb += kTile) {
             const uint32_t m = static_cast<uint32_t>(min(static_cast<unsigned long long>(kTile), re - cb));
@@ -637,31 +673,32 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                 fullrow[tid] = p != kNone && set_size[p] == static_cast<uint32_t>(K) ? 1u : 0u;
             }
             __syncthreads();
-            // The chunk's rows (and S(q)'s for a new q): one bulk copy per row.
-            if (warp == 0) {
-                if (lane == 0) tc::mbar_arrive_expect_tx(&rows_bar, (m + (with_b ? nc : 0u)) * kRowBytes);
+            JOIN_MARK(2)
+            // S(q)'s rows for a new q: one bulk copy per row; meanwhile the
+            // chunk's rows are converted straight from global memory.
+            if (with_b && warp == 0) {
+                tc::fence_proxy_async();  // the last q's reads of rows_b come before these writes
+                if (lane == 0) tc::mbar_arrive_expect_tx(&rows_bar, nc * kRowBytes);
                 __syncwarp();
-                for (uint32_t r = lane; r < m; r += kWarp)
-                    tc::bulk_g2s(rows_a + static_cast<size_t>(r) * D, pts + static_cast<size_t>(pid[r]) * ld, kRowBytes,
+                for (uint32_t j = lane; j < nc; j += kWarp)
+                    tc::bulk_g2s(rows_b + static_cast<size_t>(j) * D, pts + static_cast<size_t>(cid[j]) * ld, kRowBytes,
                                  &rows_bar);
-                if (with_b)
-                    for (uint32_t j = lane; j < nc; j += kWarp)
-                        tc::bulk_g2s(rows_b + static_cast<size_t>(j) * D, pts + static_cast<size_t>(cid[j]) * ld,
-                                     kRowBytes, &rows_bar);
             }
-            if (!wait_or_fail(&rows_bar, ph_rows)) {
-                healthy = false;
-                break;
-            }
-            ph_rows ^= 1u;
             // Centred FP16 operand tiles, norms and error terms.
-            if (tid < 2 * kTile)
-                convert_rows<D>(rows_a, m, kTile, tile_a, centre, normA, rtA, tid);
-            else
-                convert_rows<D>(rows_b, nc, NB, tile_b, centre, normB, rtB, tid - 2 * kTile);
+            convert_rows<D, true>(pts, pid, static_cast<size_t>(ld), m, kTile, tile_a, centre, normA, rtA, tid);
+            if (with_b) {
+                if (!wait_or_fail(&rows_bar, ph_rows)) {
+                    healthy = false;
+                    break;
+                }
+                ph_rows ^= 1u;
+            }
+            JOIN_MARK(3)
+            convert_rows<D, false>(rows_b, nullptr, static_cast<size_t>(D), nc, NB, tile_b, centre, normB, rtB, tid);
             tc::fence_proxy_async();
             tc::fence_before_sync();
             __syncthreads();
+            JOIN_MARK(4)
             if (tid == 0) {
                 tc::fence_after_sync();
                 tc::issue_tile_16bit(tmem, tc::smem_u32(tile_a), tc::smem_u32(tile_b), kTile, NB, L::KP, idesc);
@@ -672,6 +709,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                 break;
             }
             ph_mma ^= 1u;
+            JOIN_MARK(5)
             tc::fence_after_sync();
             // The tiles are consumed: the chunk's lists S(p) go into their space
             // (one bulk copy per list) while the filter runs.
@@ -682,7 +720,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                     tc::bulk_g2s(lists + static_cast<size_t>(r) * KS, snap + static_cast<size_t>(pid[r]) * K,
                                  static_cast<uint32_t>(K) * 4u, &list_bar);
             }
-            // Filter: bit u of `todo` marks column group*32 + u as a pair that
+            // Filter: bit u of `todo` marks column group*64 + u as a pair that
             // may beat bound(p).
             const uint32_t p = row < static_cast<int>(m) ? pid[row] : kNone;
             const float bp = row < static_cast<int>(m) ? bnd[row] : 0.0f;
@@ -691,9 +729,9 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                 const float na = normA[row], ra = rtA[row];
                 const int j0 = group * kGroupCols;
                 if (j0 < static_cast<int>(nc)) {  // warp-uniform
-                    uint32_t pass = 0;
+                    unsigned long long pass = 0;
 #pragma unroll
-                    for (int hh = 0; hh < 2; ++hh) {
+                    for (int hh = 0; hh < kGroupCols / 16; ++hh) {
                         const int jb = j0 + 16 * hh;
                         if (jb >= static_cast<int>(nc)) break;  // warp-uniform
                         float g[16];
@@ -706,15 +744,15 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                             const float margin = 0.00390625f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + ra +
                                                  rtB[jb + u];
                             // NaN-safe: a pair is dropped only when the bound provably holds.
-                            if (!(approx - margin >= bp)) pass |= 1u << (16 * hh + u);
+                            if (!(approx - margin >= bp)) pass |= 1ull << (16 * hh + u);
                         }
                     }
                     const int valid_cols = max(0, min(kGroupCols, static_cast<int>(nc) - j0));
-                    pass &= valid_cols == kGroupCols ? 0xFFFFFFFFu : ((1u << valid_cols) - 1u);
+                    pass &= valid_cols == kGroupCols ? ~0ull : ((1ull << valid_cols) - 1ull);
                     if (p == kNone) pass = 0;
                     if (p != kNone) {
                         n_pairs += valid_cols;
-                        n_pass += __popc(pass);
+                        n_pass += __popcll(pass);
                     }
                     todo = pass;
                 }
@@ -744,10 +782,12 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
             // (branch-free, in lockstep).  A set that is not full lists its
             // empty slots as its point set's first id (0 for a single set),
             // which is then its list's first entry and not taken for a member.
+            JOIN_MARK(6)
             todo_s[tid] = todo;
             mem_s[tid] = 0ull;
             uint32_t incl = scan_masks_warp(todo, wsum);
             __syncthreads();
+            JOIN_MARK(7)
             scan_masks_block(todo, incl, wsum, pref);
             if (bulk_lists && !wait_or_fail(&list_bar, ph_list)) {
                 healthy = false;
@@ -755,6 +795,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
             }
             if (bulk_lists) ph_list ^= 1u;
             __syncthreads();
+            JOIN_MARK(8)
             {
                 PairCursor cur = pair_share(pref, todo_s);
 #pragma unroll 1
@@ -793,6 +834,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                 }
             }
             __syncthreads();
+            JOIN_MARK(9)
             // The remaining pairs, an even share per thread: exact distances
             // from the staged original rows.
             todo &= ~mem_s[tid];
@@ -801,6 +843,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
             __syncthreads();
             scan_masks_block(todo, incl, wsum, pref);
             __syncthreads();
+            JOIN_MARK(10)
             {
                 PairCursor cur = pair_share(pref, todo_s);
 #pragma unroll 1
@@ -813,8 +856,9 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
                     const uint32_t c = cid[j];
                     if (c == pp) continue;
                     ++n_exact;
-                    const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(rows_b + j * D),
-                                                                reinterpret_cast<const float4*>(rows_a + prow * D));
+                    const float d = canonical_distance4_lean<D>(
+                        reinterpret_cast<const float4*>(rows_b + j * D),
+                        reinterpret_cast<const float4*>(pts + static_cast<size_t>(pp) * ld));
                     if (d < bnd[prow]) {
                         ++n_emit;
                         const uint32_t s = atomicAdd(&surv_count[pp], 1u);
@@ -836,9 +880,14 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
             // next chunk's copies and MMA.
             tc::fence_before_sync();
             __syncthreads();
+            JOIN_MARK(11)
             tc::fence_after_sync();
         }
     }
+#ifdef KNNG_JOIN_PHASES
+    if (tid == 0)
+        for (int i = 0; i < kJoinPhases; ++i) atomicAdd(&counters[8 + i], static_cast<unsigned long long>(ph_[i]));
+#endif
     atomicAdd(&counters[0], n_pairs);
     atomicAdd(&counters[1], n_pass);
     atomicAdd(&counters[2], n_member);
@@ -951,8 +1000,6 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     using L = JoinLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
     const JoinSmem S = join_smem(D, kTile);
-    float* rows_a = reinterpret_cast<float*>(smem + S.rows_a);
-    float* rows_b = reinterpret_cast<float*>(smem + S.rows_b);
     unsigned char* tile_a = smem + S.tiles;
     unsigned char* tile_b = smem + S.tile_b;
     float* norm_a = reinterpret_cast<float*>(smem + S.norm_a);
@@ -963,8 +1010,6 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
-    for (uint32_t f = tid; f < m * D; f += kJoinThreads) rows_a[f] = a[f];
-    for (uint32_t f = tid; f < n * D; f += kJoinThreads) rows_b[f] = b[f];
     for (int j = tid; j < D; j += kJoinThreads) zero[j] = 0.0f;
     if (warp == 0) tc::tmem_alloc(&tmem_slot, kTile);
     if (tid == 0) {
@@ -975,10 +1020,9 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    if (tid < 2 * kTile)
-        convert_rows<D>(rows_a, m, kTile, tile_a, zero, norm_a, rt_a, tid);
-    else
-        convert_rows<D>(rows_b, n, kTile, tile_b, zero, norm_b, rt_b, tid - 2 * kTile);
+    __syncthreads();
+    convert_rows<D, false>(a, nullptr, static_cast<size_t>(D), m, kTile, tile_a, zero, norm_a, rt_a, tid);
+    convert_rows<D, false>(b, nullptr, static_cast<size_t>(D), n, kTile, tile_b, zero, norm_b, rt_b, tid);
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
@@ -995,7 +1039,7 @@ __global__ void __launch_bounds__(kJoinThreads, 1)
     } else {
         tc::fence_after_sync();
         const int quarter = warp % 4, group = warp / 4, row = quarter * kWarp + lane;
-        for (int hh = 0; hh < 2; ++hh) {
+        for (int hh = 0; hh < kGroupCols / 16; ++hh) {
             const int j0 = group * kGroupCols + 16 * hh;
             float g[16];
             tc::tmem_ld16(tmem + (static_cast<uint32_t>(quarter * kWarp) << 16) + j0, g);
@@ -1147,7 +1191,7 @@ uint64_t run_refine(Context& c) {
     c.launches += 2;
     KNNG_CUDA(cudaGetLastError());
 
-    // Join grid: one persistent CTA per SM; each owns one pool region.
+    // Join grid: kJoinPerSm persistent CTAs per SM; each owns one pool region.
     const uint32_t join_bytes = join_smem(static_cast<int>(c.d), static_cast<uint32_t>(K)).bytes;
     // CTAs per SM from the SM's shared memory and registers (the kernel's
     // launch bounds ask for two).
@@ -1167,7 +1211,7 @@ uint64_t run_refine(Context& c) {
     const size_t per_cta_smem = join_bytes + fa.sharedSizeBytes + static_cast<size_t>(smem_reserved);
     const int by_smem = static_cast<int>(static_cast<size_t>(smem_sm) / per_cta_smem);
     const int by_regs = fa.numRegs > 0 ? regs_sm / (fa.numRegs * kJoinThreads) : 2;
-    const int per_sm = std::min({by_smem, by_regs, 1});
+    const int per_sm = std::min({by_smem, by_regs, kJoinPerSm});
     if (per_sm < 1) fail(KNNG_ERR_UNSUPPORTED, "the join kernel does not fit on an SM");
     const uint32_t kJoinBlocks = static_cast<uint32_t>(sms) * static_cast<uint32_t>(per_sm);
     // Survivor storage: `slots` per point, then per-CTA pool regions for the
@@ -1201,7 +1245,7 @@ uint64_t run_refine(Context& c) {
         scratch(c, "surv_offsets", (static_cast<size_t>(n) + 1) * sizeof(unsigned long long)));
     auto* pool_fill = static_cast<uint32_t*>(scratch(c, "surv_pool_fill", kJoinBlocks * sizeof(uint32_t)));
     auto* err = static_cast<uint32_t*>(scratch(c, "join_error", sizeof(uint32_t)));
-    auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 8 * sizeof(unsigned long long)));
+    auto* jc = static_cast<unsigned long long*>(scratch(c, "join_counters", 24 * sizeof(unsigned long long)));
     auto* counters = static_cast<uint32_t*>(scratch(c, "apply_counters", 4 * sizeof(uint32_t)));
     auto* work = static_cast<uint32_t*>(scratch(c, "join_work", sizeof(uint32_t)));
     auto* big = static_cast<uint32_t*>(scratch(c, "apply_big", static_cast<size_t>(n) * sizeof(uint32_t)));
@@ -1216,7 +1260,7 @@ uint64_t run_refine(Context& c) {
     KNNG_CUDA(cudaMemsetAsync(ofill, 0, static_cast<size_t>(n) * sizeof(uint32_t), c.stream));
     KNNG_CUDA(cudaMemsetAsync(lost, 0, n, c.stream));
     KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
-    KNNG_CUDA(cudaMemsetAsync(jc, 0, 8 * sizeof(unsigned long long), c.stream));
+    KNNG_CUDA(cudaMemsetAsync(jc, 0, 24 * sizeof(unsigned long long), c.stream));
     KNNG_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), c.stream));
     KNNG_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), c.stream));
     // Points in the leaf order of the last repetition (c.indices), unless the
@@ -1304,9 +1348,20 @@ uint64_t run_refine(Context& c) {
         cudaEventDestroy(r2);
     }
     uint32_t h[2] = {0, 0};
-    unsigned long long hc[8] = {0};
+    unsigned long long hc[24] = {0};
     download(c, h, counters, 2);
-    download(c, hc, jc, 8);
+    download(c, hc, jc, 24);
+#ifdef KNNG_JOIN_PHASES
+    {
+        static const char* names[] = {"fetch", "columns", "chunk_setup", "rows_wait", "convert", "mma",
+                                      "filter",  "scan1",   "lists_wait",  "member",    "scan2",   "exact"};
+        double tot = 0;
+        for (int i = 0; i < 12; ++i) tot += static_cast<double>(hc[8 + i]);
+        fprintf(stderr, "join phases:");
+        for (int i = 0; i < 12; ++i) fprintf(stderr, " %s=%.3f", names[i], hc[8 + i] / std::max(tot, 1.0));
+        fprintf(stderr, "\n");
+    }
+#endif
     uint64_t changed = h[1] + changed_lost;
     KNNG_CUDA(cudaEventSynchronize(ev[3]));
     const float ms_all = elapsed(ev[0], ev[3]);
