@@ -326,10 +326,13 @@ __host__ __device__ constexpr uint32_t list_stride(uint32_t K) { return (K & 3u)
 
 // Dynamic shared memory of k_join (byte offsets).  rows_b: the original FP32
 // rows of S(q), row-major, bulk-copied once per q; they feed the centred B'
-// tile and the column side of the exact distances (the rows of R(q) are read
-// from global memory, so that two CTAs fit an SM).  tiles: the A' and B'
-// operand tiles, and once the MMA has read them the lists S(p) of the chunk's
-// rows.  x: per-thread pair masks, member masks, prefix sums.
+// tile and the column side of the exact distances.  tiles: one region used
+// three times per chunk: the A' and B' operand tiles (A' converted straight
+// from the rows of R(q) in global memory), once the MMA has read them the
+// lists S(p) of the chunk's rows, and once the member searches are done the
+// chunk's original rows (the row side of the exact distances).  Keeping only
+// S(q)'s rows resident lets two CTAs share an SM.  x: per-thread pair masks,
+// member masks, prefix sums.
 struct JoinSmem {
     uint32_t rows_b, tiles, tile_b, norm_a, norm_b, rt_a, rt_b, bnd, pid, cid, fullrow, centre, x, bytes;
 };
@@ -343,7 +346,10 @@ __host__ __device__ inline JoinSmem join_smem(int D, uint32_t K) {
     s.rows_b = 0;
     s.tiles = (s.rows_b + NB * static_cast<uint32_t>(D) * 4 + 127) / 128 * 128;
     s.tile_b = s.tiles + kTile * KP * 2;
-    s.norm_a = s.tiles + ((tiles_bytes > lists_bytes ? tiles_bytes : lists_bytes) + 15) / 16 * 16;
+    const uint32_t rows_bytes = kTile * static_cast<uint32_t>(D) * 4;
+    uint32_t region = tiles_bytes > lists_bytes ? tiles_bytes : lists_bytes;
+    region = region > rows_bytes ? region : rows_bytes;
+    s.norm_a = s.tiles + (region + 15) / 16 * 16;
     s.norm_b = s.norm_a + kTile * 4;
     s.rt_a = s.norm_b + kTile * 4;
     s.rt_b = s.rt_a + kTile * 4;
@@ -580,7 +586,7 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
     unsigned long long* mem_s = todo_s + kJoinThreads;                                // [kJoinThreads]
     uint32_t* pref = reinterpret_cast<uint32_t*>(smem + S.x + 2 * kJoinThreads * 8);  // [kJoinThreads + 1]
     uint32_t* wsum = pref + kJoinThreads + 1;                                          // [kJoinWarps]
-    __shared__ uint64_t rows_bar, list_bar, mma_bar;
+    __shared__ uint64_t rows_bar, list_bar, mma_bar, arow_bar;
     __shared__ uint32_t tmem_slot;
     __shared__ uint32_t ncols_s;
     __shared__ uint32_t pool_cursor;
@@ -592,6 +598,7 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
         tc::mbar_init(&rows_bar, 1);
         tc::mbar_init(&list_bar, 1);
         tc::mbar_init(&mma_bar, 1);
+        tc::mbar_init(&arow_bar, 1);
         tc::fence_barrier_init();
     }
     tc::fence_before_sync();
@@ -602,7 +609,8 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
     const bool bulk_lists = (K & 3) == 0;
     const int KS = static_cast<int>(list_stride(static_cast<uint32_t>(K)));
     constexpr uint32_t kRowBytes = D * sizeof(float);
-    uint32_t ph_rows = 0, ph_list = 0, ph_mma = 0;
+    uint32_t ph_rows = 0, ph_list = 0, ph_mma = 0, ph_arow = 0;
+    float* arows = reinterpret_cast<float*>(smem + S.tiles);  // the chunk's R(q) rows, for the exact phase
     bool healthy = true;
     unsigned long long n_pairs = 0, n_pass = 0, n_member = 0, n_exact = 0, n_emit = 0;
     const int quarter = warp % 4, group = warp / 4;
@@ -835,6 +843,16 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
             }
             __syncthreads();
             JOIN_MARK(9)
+            // The lists are consumed: the chunk's original rows go into their
+            // space (one bulk copy per row; recently read, mostly from L2).
+            if (warp == 0) {
+                tc::fence_proxy_async();  // the searches' reads of the lists come before these writes
+                if (lane == 0) tc::mbar_arrive_expect_tx(&arow_bar, m * kRowBytes);
+                __syncwarp();
+                for (uint32_t r = lane; r < m; r += kWarp)
+                    tc::bulk_g2s(arows + static_cast<size_t>(r) * D, pts + static_cast<size_t>(pid[r]) * ld, kRowBytes,
+                                 &arow_bar);
+            }
             // The remaining pairs, an even share per thread: exact distances
             // from the staged original rows.
             todo &= ~mem_s[tid];
@@ -843,6 +861,11 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
             __syncthreads();
             scan_masks_block(todo, incl, wsum, pref);
             __syncthreads();
+            if (!wait_or_fail(&arow_bar, ph_arow)) {
+                healthy = false;
+                break;
+            }
+            ph_arow ^= 1u;
             JOIN_MARK(10)
             {
                 PairCursor cur = pair_share(pref, todo_s);
@@ -856,9 +879,8 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
                     const uint32_t c = cid[j];
                     if (c == pp) continue;
                     ++n_exact;
-                    const float d = canonical_distance4_lean<D>(
-                        reinterpret_cast<const float4*>(rows_b + j * D),
-                        reinterpret_cast<const float4*>(pts + static_cast<size_t>(pp) * ld));
+                    const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(rows_b + j * D),
+                                                                reinterpret_cast<const float4*>(arows + prow * D));
                     if (d < bnd[prow]) {
                         ++n_emit;
                         const uint32_t s = atomicAdd(&surv_count[pp], 1u);
@@ -1314,13 +1336,16 @@ uint64_t run_refine(Context& c) {
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     if (max_count > static_cast<uint32_t>(kApplyCap)) {
-        // Each block's warps sort in big_cap keys of global scratch: fewer
-        // blocks (a longer grid stride) when the budget leaves less room.
+        // Each block's warps sort in big_cap keys of global scratch, which
+        // stays within half of L2 (the sorts make many passes over it): one
+        // block per SM at most, fewer (a longer grid stride) for large lists
+        // or when the budget leaves less room.
         const uint64_t per_block = static_cast<uint64_t>(kRefWarps) * big_cap * sizeof(unsigned long long);
         const uint64_t held_other = c.held - scratch_bytes(c, "apply_big_keys");
         const uint64_t room = c.budget > held_other + (16ull << 20) ? c.budget - held_other - (16ull << 20) : 0;
-        const uint32_t big_blocks =
-            static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(kJoinBlocks, room / per_block)));
+        const uint64_t l2_half = 60ull << 20;
+        const uint32_t big_blocks = static_cast<uint32_t>(std::max<uint64_t>(
+            1, std::min<uint64_t>({static_cast<uint64_t>(sms), room / per_block, l2_half / per_block})));
         auto* big_keys = static_cast<unsigned long long*>(
             scratch(c, "apply_big_keys", static_cast<size_t>(big_blocks) * per_block));
         k_apply_big<<<big_blocks, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, slots, direct, soff, ovf,
