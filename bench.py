@@ -214,6 +214,18 @@ def reference_prefix(n: int, m: int) -> np.ndarray:
     return workloads.subspace_mixture(max(m, min(n, 1_000_000)), seed=SEED)[:m]
 
 
+def host_cpu_model() -> str:
+    """The host CPU's model name (first processor in /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def reference_sample_rate(n: int, reps: int, passes: int, target_s: float, steps: int, warmup: int):
     """Times the reference's own code (all host threads) on a prefix of the
     point set: each step = `reps` repetitions of splitKmeansBinaryProcess
@@ -277,7 +289,7 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(args.n, args.reps, args.refine, MAX_LEAF, False, args.gpus),
             "cpu_baseline": {"value": value, "unit": "points/s", "cores": res["cores"], "kind": "reference",
-                             "sample": sample},
+                             "cpu": host_cpu_model(), "sample": sample},
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line))
@@ -755,7 +767,7 @@ def run_ours(args):
             if res:
                 line["cpu_baseline"] = {
                     "value": sig(res["rates"][0]), "unit": "points/s", "cores": res["cores"], "kind": "reference",
-                    "sample": f"reference splitKmeansBinaryProcess x{args.reps} + topUpSingle x{args.refine}, all host "
+                    "cpu": host_cpu_model()[:48], "sample": f"reference splitKmeansBinaryProcess x{args.reps} + topUpSingle x{args.refine}, all host "
                               f"threads, first {res['sample_points']:,} points of the same set"}
         except Exception as e:  # the baseline must not hide the GPU number
             line["cpu_baseline"] = {"error": str(e)[:200]}

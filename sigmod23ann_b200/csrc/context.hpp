@@ -99,6 +99,10 @@ struct Context {
     // The join takes points in the leaf order of the last repetition; true
     // (environment KNNG_JOIN_ORDER=id at creation): in id order.
     bool join_order_ids = false;
+    // FP32 bucket pass: distances only where the tensor-core filter cannot
+    // rule a pair out (k_leaf_tc); false (environment KNNG_LEAF=fp32 at
+    // creation): every pair's distance (k_leaf).  Both give the same sets.
+    bool leaf_tc = true;
     int64_t refine_pool = -1;
     // Breakdown of the last refinement pass.
     struct RefineRecord {
@@ -218,9 +222,10 @@ uint32_t start_count(uint32_t n);
 void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
                    uint32_t max_bucket, uint64_t* evals);
 // Persistent bucket pass over a device list of *d_count buckets taken from
-// the work counter *d_work (zeroed beforehand).
+// the work counter *d_work (zeroed beforehand); *d_error is set when a
+// tensor-core wait gives up.
 void launch_leaves_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
-                        uint32_t* d_work, uint32_t max_bucket);
+                        uint32_t* d_work, uint32_t max_bucket, uint32_t* d_error);
 void launch_leaves_bf16_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
                              uint32_t* d_work, uint32_t* d_error);
 // Exact k nearest points (FP32 distances in the reference's order) of the

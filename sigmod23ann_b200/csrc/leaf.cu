@@ -11,6 +11,9 @@
 // memory tiles, then each warp replays its points' 64 offers in column order
 // (set_offer_batch).  Distances are computed for the full b x b matrix (both
 // triangles); each (i, j) and (j, i) evaluation gives the same bits.
+// k_leaf_tc (the default) makes the same offers but computes distances only
+// for the pairs a tensor-core filter cannot rule out (see below).
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -19,6 +22,7 @@
 #include "common.cuh"
 #include "context.hpp"
 #include "dispatch.hpp"
+#include "tc.cuh"
 
 namespace knng {
 namespace {
@@ -309,6 +313,297 @@ __global__ void k_sample_recall(const uint32_t* __restrict__ queries, uint32_t n
     if (lane == 0 && mine) atomicAdd(hits, static_cast<unsigned long long>(mine));
 }
 
+// ------------------------------------------- bucket pass, tensor-core filter
+//
+// The same offers in the same order as k_leaf, with the distances of pairs
+// that cannot be accepted left out.  Per 64 x 64 block (row block I, column
+// block J) the rows, centred on the bucket's first point and rounded to FP16,
+// are multiplied on the tensor cores (tcgen05.mma kind::f16, FP32
+// accumulation; the A tile has 128 rows, the row block's 64 and zeros):
+// approx = |x'|^2 + |y'|^2 - 2 x'.y'.  A pair is left out when
+// approx - margin >= bound(p) at the start of the column block, with the
+// margin of the neighbour-of-neighbour join's filter
+//   2^-8 (|x'|^2 + |y'|^2) + 2^-16 |approx| + 2^-19 (|x'| + |y'|)
+// (+inf for a row with a value outside FP16's range): its FP32 distance is
+// then >= the bound at the time of its offer (bounds only fall), so the
+// reference rejects it too.  The other pairs of each row are compacted in
+// column order, their exact distances computed in the reference's FP32 order
+// from the dim-major FP32 tiles, and offered through the same warp-resident
+// set update.  While a set is not full its bound is FLT_MAX and nothing is
+// left out.
+
+constexpr int kTcRows = 128;  // MMA M: the A tile's rows
+
+template <int D>
+struct LeafTc {
+    static constexpr int KP = (D + 15) / 16 * 16;  // K padded to the MMA step of 16
+    static constexpr int CH = KP / 8;              // 16-byte chunks per FP16 row
+    static constexpr uint32_t I = 0;                                     // FP32 [D][kBI]
+    static constexpr uint32_t J = I + D * kBI * 4;                       // FP32 [D][kBJ]
+    static constexpr uint32_t A = (J + D * kBJ * 4 + 127) / 128 * 128;  // FP16 chunk-major, kTcRows rows
+    static constexpr uint32_t B = A + kTcRows * KP * 2;                  // FP16 chunk-major, kBJ rows
+    static constexpr uint32_t norm_a = B + kBJ * KP * 2;
+    static constexpr uint32_t rt_a = norm_a + kBI * 4;
+    static constexpr uint32_t norm_b = rt_a + kBI * 4;
+    static constexpr uint32_t rt_b = norm_b + kBJ * 4;
+    static constexpr uint32_t bnd = rt_b + kBJ * 4;         // bound of each row at the column block's start
+    static constexpr uint32_t pass = bnd + kBI * 4;         // u16 pass masks [kBI rows][4 groups of 16 columns]
+    static constexpr uint32_t cols = pass + kBI * 4 * 2;    // per warp: compacted columns of one row (u8 [kBJ])
+    static constexpr uint32_t centre = cols + kLeafWarps * kBJ;
+    static constexpr uint32_t ids = centre + (D + 3) / 4 * 16;
+    static constexpr size_t bytes(uint32_t max_bucket) {
+        return ids + static_cast<size_t>(max_bucket > 1 ? max_bucket : 1) * 4;
+    }
+};
+
+// Rows r < count of a dim-major FP32 tile (`src`, kBI == kBJ columns) minus
+// `centre`, rounded to FP16, into a chunk-major tile of R rows (chunk c of row
+// r at c*R*16 + r*16); rows past count are zeros.  Also each row's squared
+// norm (FP32 of the centred values) and absolute error term 2^-19 |x'| (+inf
+// when a value does not fit FP16).  Threads 0..127 (warps 0-3, all lanes):
+// two per row.
+template <int D>
+__device__ __forceinline__ void convert_dm(const float* __restrict__ src, uint32_t count, uint32_t R,
+                                           unsigned char* __restrict__ tile, const float* __restrict__ centre,
+                                           float* __restrict__ norm, float* __restrict__ rt, int t) {
+    constexpr int CH = LeafTc<D>::CH;
+    constexpr int HALF = (CH + 1) / 2;
+    const uint32_t r = static_cast<uint32_t>(t) >> 1;
+    const int h = t & 1;
+    const bool live = r < count;
+    float s = 0.0f, mx = 0.0f;
+#pragma unroll 1
+    for (int i = 0; i < HALF; ++i) {
+        const int c = h * HALF + i;
+        if (c >= CH) break;
+        float v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int k = 8 * c + e;
+            v[e] = live && k < D ? __fsub_rn(src[k * kBJ + r], centre[k]) : 0.0f;
+            s = fmaf(v[e], v[e], s);
+            mx = fmaxf(mx, fabsf(v[e]));
+        }
+        uint4 packed;
+        uint32_t* pk = reinterpret_cast<uint32_t*>(&packed);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const __half2 hv = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
+            pk[e] = *reinterpret_cast<const uint32_t*>(&hv);
+        }
+        *reinterpret_cast<uint4*>(tile + static_cast<size_t>(c) * R * 16 + static_cast<size_t>(r) * 16) = packed;
+    }
+    const float so = __shfl_xor_sync(kFull, s, 1);
+    const float mo = __shfl_xor_sync(kFull, mx, 1);
+    if (h == 0) {
+        const float nrm = s + so;
+        norm[r] = nrm;
+        rt[r] = fmaxf(mx, mo) >= 32768.0f ? __int_as_float(0x7f800000) : 1.9073486328125e-06f * sqrtf(nrm);
+    }
+}
+
+// Canonical FP32 distance (the reference's order) between row `i` of the
+// dim-major I tile and column `j` of the dim-major J tile; the same
+// arithmetic as distance_block.
+template <int D>
+__device__ __forceinline__ float distance_dm(const float* __restrict__ I, uint32_t i, const float* __restrict__ J,
+                                             uint32_t j) {
+    constexpr int M = D / 8 * 8;
+    float tot = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        float ch = 0.0f;
+#pragma unroll
+        for (int dim = c; dim < M; dim += 8) {
+            const float diff = __fsub_rn(I[dim * kBI + i], J[dim * kBJ + j]);
+            ch = __fmaf_rn(diff, diff, ch);
+        }
+        tot = __fadd_rn(tot, ch);
+    }
+#pragma unroll
+    for (int dim = M; dim < D; ++dim) {
+        const float diff = __fsub_rn(I[dim * kBI + i], J[dim * kBJ + j]);
+        tot = __fadd_rn(tot, __fmul_rn(diff, diff));
+    }
+    return tot;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kLeafThreads, 2)
+    k_leaf_tc(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends,
+              const uint32_t* __restrict__ idx, const float* __restrict__ pts, int ld, float* __restrict__ set_dist,
+              uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
+              float* __restrict__ set_bound, int K, const uint32_t* __restrict__ dcount, uint32_t* __restrict__ work,
+              uint32_t* __restrict__ error_flag) {
+    using L = LeafTc<D>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* I = reinterpret_cast<float*>(smem + L::I);
+    float* J = reinterpret_cast<float*>(smem + L::J);
+    unsigned char* A = smem + L::A;
+    unsigned char* Bt = smem + L::B;
+    float* norm_a = reinterpret_cast<float*>(smem + L::norm_a);
+    float* rt_a = reinterpret_cast<float*>(smem + L::rt_a);
+    float* norm_b = reinterpret_cast<float*>(smem + L::norm_b);
+    float* rt_b = reinterpret_cast<float*>(smem + L::rt_b);
+    float* bnd = reinterpret_cast<float*>(smem + L::bnd);
+    uint16_t* pass = reinterpret_cast<uint16_t*>(smem + L::pass);
+    uint8_t* cols = smem + L::cols;
+    float* centre = reinterpret_cast<float*>(smem + L::centre);
+    uint32_t* ids = reinterpret_cast<uint32_t*>(smem + L::ids);
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ uint32_t next_s;
+    const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+    const unsigned lt = (1u << lane) - 1u;
+    uint8_t* my_cols = cols + warp * kBJ;
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, kBJ);
+    if (tid == 0) {
+        tc::mbar_init(&mbar, 1);
+        tc::fence_barrier_init();
+    }
+    // A tile rows kBI..kTcRows-1 stay zero.
+    for (int f = tid; f < L::CH * (kTcRows - kBI); f += kLeafThreads) {
+        const int c = f / (kTcRows - kBI), r = kBI + f % (kTcRows - kBI);
+        *reinterpret_cast<uint4*>(A + static_cast<size_t>(c) * kTcRows * 16 + static_cast<size_t>(r) * 16) =
+            make_uint4(0u, 0u, 0u, 0u);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = tc::idesc_f16(kTcRows, kBJ);
+    uint32_t phase = 0;
+    bool healthy = true;
+    for (uint32_t round = 0; healthy; ++round) {
+        uint32_t leaf;
+        if (work) {
+            if (tid == 0) next_s = atomicAdd(work, 1u);
+            __syncthreads();
+            leaf = next_s;
+            __syncthreads();
+            if (leaf >= *dcount) break;
+        } else {
+            if (round > 0) break;
+            leaf = blockIdx.x;
+        }
+        const uint32_t s0 = starts[leaf];
+        const uint32_t b = ends[leaf] - s0;
+        if (b < 2) continue;
+        for (uint32_t t = tid; t < b; t += kLeafThreads) ids[t] = idx[s0 + t];
+        __syncthreads();
+        for (int k = tid; k < D; k += kLeafThreads) centre[k] = pts[static_cast<size_t>(ids[0]) * ld + k];
+        for (uint32_t ib = 0; ib < b && healthy; ib += kBI) {
+            __syncthreads();  // the centre is written; the last row block's readers of I are done
+            load_tile<D>(I, ids, ib, b, pts, ld);
+            WarpSet sets[kPtsPerWarp];
+#pragma unroll
+            for (int u = 0; u < kPtsPerWarp; ++u) {
+                const uint32_t row = warp * kPtsPerWarp + u;
+                const uint32_t p = ib + row;
+                if (p < b) set_load(sets[u], set_dist, set_id, set_size, set_maxslot, set_bound, ids[p], K, lane);
+                if (lane == 0) bnd[row] = p < b ? sets[u].bound : -FLT_MAX;
+            }
+            __syncthreads();
+            if (tid < 2 * kBI) convert_dm<D>(I, min(static_cast<uint32_t>(kBI), b - ib), kTcRows, A, centre, norm_a,
+                                             rt_a, tid);
+            for (uint32_t jb = 0; jb < b; jb += kBJ) {
+                __syncthreads();  // the last column block's readers of J, B and the masks are done
+                load_tile<D>(J, ids, jb, b, pts, ld);
+                __syncthreads();
+                if (tid < 2 * kBJ)
+                    convert_dm<D>(J, min(static_cast<uint32_t>(kBJ), b - jb), kBJ, Bt, centre, norm_b, rt_b, tid);
+                tc::fence_proxy_async();
+                tc::fence_before_sync();
+                __syncthreads();
+                if (tid == 0) {
+                    tc::fence_after_sync();
+                    tc::issue_tile_16bit(tmem, tc::smem_u32(A), tc::smem_u32(Bt), kTcRows, kBJ, L::KP, idesc);
+                    tc::mma_commit(&mbar);
+                }
+                // Thread 0 polls; the others wait in the barrier.
+                const bool done = tid == 0 ? tc::mbar_wait_limited(&mbar, phase) : true;
+                phase ^= 1u;
+                if (__syncthreads_or(!done)) {
+                    if (tid == 0) {
+                        atomicExch(error_flag, 1u);
+                        tc::mbar_wait(&mbar, phase ^ 1u);
+                    }
+                    healthy = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                // Filter: warps whose TMEM lane quarter holds rows 0..63 read
+                // 16 accumulator columns each.
+                if ((warp & 3) < kBI / kWarp) {
+                    const int row = (warp & 3) * kWarp + lane;
+                    const int g0 = (warp >> 2) * 16;
+                    float g[16];
+                    tc::tmem_ld16(tmem + (static_cast<uint32_t>((warp & 3) * kWarp) << 16) + g0, g);
+                    tc::tmem_wait_ld();
+                    const float na = norm_a[row], ra = rt_a[row], bp = bnd[row];
+                    uint32_t m = 0;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const float nb = norm_b[g0 + u];
+                        const float approx = na + nb - 2.0f * g[u];
+                        const float margin = 0.00390625f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + ra +
+                                             rt_b[g0 + u];
+                        // NaN-safe: a pair is left out only when the bound provably holds.
+                        if (!(approx - margin >= bp)) m |= 1u << u;
+                    }
+                    pass[row * 4 + (warp >> 2)] = static_cast<uint16_t>(m);
+                }
+                tc::fence_before_sync();
+                __syncthreads();
+                // Offers: each warp its four rows, the passing columns in order.
+#pragma unroll
+                for (int u = 0; u < kPtsPerWarp; ++u) {
+                    const uint32_t row = warp * kPtsPerWarp + u;
+                    const uint32_t p = ib + row;
+                    if (p >= b) continue;  // warp-uniform
+                    const uint32_t ncols = min(static_cast<uint32_t>(kBJ), b - jb);
+                    unsigned long long m = static_cast<unsigned long long>(pass[row * 4 + 0]) |
+                                           static_cast<unsigned long long>(pass[row * 4 + 1]) << 16 |
+                                           static_cast<unsigned long long>(pass[row * 4 + 2]) << 32 |
+                                           static_cast<unsigned long long>(pass[row * 4 + 3]) << 48;
+                    if (ncols < 64) m &= (1ull << ncols) - 1ull;
+                    if (p >= jb && p < jb + kBJ) m &= ~(1ull << (p - jb));
+                    uint32_t n = 0;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const bool bit = (m >> (h * kWarp + lane)) & 1ull;
+                        const unsigned bal = __ballot_sync(kFull, bit);
+                        if (bit) my_cols[n + __popc(bal & lt)] = static_cast<uint8_t>(h * kWarp + lane);
+                        n += __popc(bal);
+                    }
+                    __syncwarp();
+                    for (uint32_t t0 = 0; t0 < n; t0 += kWarp) {
+                        const bool valid = t0 + lane < n;
+                        const uint32_t j = valid ? my_cols[t0 + lane] : 0u;
+                        const float d = valid ? distance_dm<D>(I, row, J, j) : 0.0f;
+                        const uint32_t cand = valid ? ids[jb + j] : 0u;
+                        set_offer_batch(sets[u], cand, d, valid, K, lane);
+                    }
+                    __syncwarp();
+                    if (lane == 0) bnd[row] = sets[u].bound;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kPtsPerWarp; ++u) {
+                const uint32_t p = ib + warp * kPtsPerWarp + u;
+                if (p < b) set_store(sets[u], set_dist, set_id, set_size, set_maxslot, set_bound, ids[p], K, lane);
+            }
+        }
+        __syncthreads();  // every warp is done with ids before the next bucket
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, kBJ);
+    }
+}
+
 }  // namespace
 
 void sample_knn(Context& c, const uint32_t* d_queries, uint32_t nq, uint32_t* d_truth) {
@@ -353,6 +648,26 @@ double sample_recall(Context& c, const uint32_t* d_queries, uint32_t nq, const u
 void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const uint32_t* d_ends,
                    uint32_t max_bucket, uint64_t* evals) {
     if (count == 0) return;
+    (void)evals;
+    if (c.leaf_tc) {
+        auto* err = static_cast<uint32_t*>(scratch(c, "leaf_error", sizeof(uint32_t)));
+        KNNG_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), c.stream));
+        KNNG_DISPATCH_D(c.d, {
+            const size_t smem = LeafTc<D>::bytes(max_bucket);
+            if (smem > 227 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "bucket too large for the bucket kernel");
+            auto kern = k_leaf_tc<D>;
+            allow_max_smem(c, kern);
+            kern<<<count, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
+                                                          c.set_id, c.set_size, c.set_maxslot, c.set_bound,
+                                                          static_cast<int>(c.k), nullptr, nullptr, err);
+        });
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
+        uint32_t h = 0;
+        download(c, &h, err, 1);
+        if (h) fail(KNNG_ERR_CUDA, "bucket pass: the MMA completion wait gave up");
+        return;
+    }
     KNNG_DISPATCH_D(c.d, {
         const size_t smem = static_cast<size_t>(D) * (kBI + kBJ) * sizeof(float) +
                             static_cast<size_t>(kBI) * kDmStride * sizeof(float) +
@@ -366,15 +681,33 @@ void launch_leaves(Context& c, uint32_t count, const uint32_t* d_starts, const u
     });
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
-    (void)evals;
 }
 
 void prepare_leaves_list(Context& c) {
-    KNNG_DISPATCH_D(c.d, { allow_max_smem(c, k_leaf<D>); });
+    KNNG_DISPATCH_D(c.d, {
+        allow_max_smem(c, k_leaf<D>);
+        allow_max_smem(c, k_leaf_tc<D>);
+    });
 }
 
 void launch_leaves_list(Context& c, const uint32_t* d_starts, const uint32_t* d_ends, const uint32_t* d_count,
-                        uint32_t* d_work, uint32_t max_bucket) {
+                        uint32_t* d_work, uint32_t max_bucket, uint32_t* d_error) {
+    if (c.leaf_tc) {
+        KNNG_DISPATCH_D(c.d, {
+            const size_t smem = LeafTc<D>::bytes(max_bucket);
+            if (smem > 227 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "bucket too large for the bucket kernel");
+            auto kern = k_leaf_tc<D>;
+            allow_max_smem(c, kern);
+            // Persistent: two CTAs per SM take the buckets from the work counter.
+            kern<<<2 * c.sms, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld,
+                                                              c.set_dist, c.set_id, c.set_size, c.set_maxslot,
+                                                              c.set_bound, static_cast<int>(c.k), d_count, d_work,
+                                                              d_error);
+        });
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
+        return;
+    }
     KNNG_DISPATCH_D(c.d, {
         const size_t smem = static_cast<size_t>(D) * (kBI + kBJ) * sizeof(float) +
                             static_cast<size_t>(kBI) * kDmStride * sizeof(float) +

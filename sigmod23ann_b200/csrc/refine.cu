@@ -625,11 +625,17 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
     // Waits on this CTA's own copies and MMAs; a wait that gives up marks the
     // launch failed, and waits once more with the full limit (the copies in
     // flight land before the CTA exits).
+    // Thread 0 alone polls; the others wait in the barrier, which takes no
+    // issue slots from the CTA sharing the SM (the barrier also makes the
+    // completed copies visible to them).
     auto wait_or_fail = [&](uint64_t* bar, uint32_t parity) -> bool {
-        const bool done = tc::mbar_wait_limited(bar, parity);
+        const bool done = tid == 0 ? tc::mbar_wait_limited(bar, parity) : true;
         if (__syncthreads_or(!done)) {
-            if (tid == 0) atomicExch(error_flag, 1u);
-            tc::mbar_wait(bar, parity);
+            if (tid == 0) {
+                atomicExch(error_flag, 1u);
+                tc::mbar_wait(bar, parity);
+            }
+            __syncthreads();
             return false;
         }
         return true;

@@ -1258,7 +1258,8 @@ void enqueue_buckets(Context& c, DevRep& r, uint32_t max_leaf, uint32_t precisio
         launch_leaves_bf16_list(c, r.leaf_start, r.leaf_end, &r.cnt->leaves, &r.cnt->leaf_work,
                                 reinterpret_cast<uint32_t*>(r.error + 1));
     else
-        launch_leaves_list(c, r.leaf_start, r.leaf_end, &r.cnt->leaves, &r.cnt->leaf_work, max_leaf - 1);
+        launch_leaves_list(c, r.leaf_start, r.leaf_end, &r.cnt->leaves, &r.cnt->leaf_work, max_leaf - 1,
+                           reinterpret_cast<uint32_t*>(r.error + 1));
 }
 
 // The repetition as one graph: prologue, WHILE (nodes left) { level },
@@ -1399,7 +1400,7 @@ void run_rep_device(Context& c, uint32_t max_leaf, uint32_t lloyd_iters, uint32_
     int32_t err[4] = {0, 0, 0, 0};
     download(c, err, r.error, 4);
     if (err[0]) fail(KNNG_ERR_CUDA, "Lloyd sums: a bulk-copy wait gave up");
-    if (err[1]) fail(KNNG_ERR_CUDA, "BF16 bucket pass: the MMA completion wait gave up");
+    if (err[1]) fail(KNNG_ERR_CUDA, "bucket pass: the MMA completion wait gave up");
     if (err[2]) fail(KNNG_ERR_CUDA, "tree levels: the level loop ran past its iteration limit");
     out.leaf_start.resize(h.leaves);
     out.leaf_end.resize(h.leaves);

@@ -465,3 +465,35 @@ def test_rep_graph_equals_other_level_loops(knng_lib, monkeypatch, loop):
     for s in range(len(sets)):
         np.testing.assert_array_equal(g_ids[s], o_ids[s])
         np.testing.assert_array_equal(g_d[s].view(np.uint32), o_d[s].view(np.uint32))
+
+
+@pytest.mark.parametrize("loop", [None, "host"])
+def test_filtered_bucket_pass_equals_plain(knng_lib, monkeypatch, loop):
+    """The bucket pass that computes distances only for pairs its tensor-core
+    filter cannot rule out (the default) leaves the same sets, bit for bit, as
+    the pass that computes every pair's distance (KNNG_LEAF=fp32): over
+    repetitions whose sets start empty, fill, and then reject most offers,
+    with buckets up to 1,024 points, in the graph and in the host level loop."""
+    pts = workloads.gaussian_mixture(n=40_000, d=100, clusters=24, sigma=0.2, seed=33)
+    if loop is None:
+        monkeypatch.delenv("KNNG_REP_LOOP", raising=False)
+    else:
+        monkeypatch.setenv("KNNG_REP_LOOP", loop)
+
+    def run(leaf):
+        if leaf is None:
+            monkeypatch.delenv("KNNG_LEAF", raising=False)
+        else:
+            monkeypatch.setenv("KNNG_LEAF", leaf)
+        out = []
+        with KnngContext(0) as c:
+            c.load_points(pts)
+            c.reset_sets(100)
+            for r, max_leaf in enumerate([1025, 257, 1025]):
+                c.run_rep(max_leaf, 2, 3000, seed=13, rep_index=r)
+                out.append(c.sets())
+        return out
+
+    filtered, plain = run(None), run("fp32")
+    for r, (a, b) in enumerate(zip(filtered, plain)):
+        assert_sets_equal(a, b, f"rep {r}")
