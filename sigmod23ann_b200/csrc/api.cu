@@ -698,7 +698,7 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     if (const char* r = std::getenv("KNNG_REFINE")) c->refine_mode = std::strcmp(r, "pointwise") == 0 ? 1 : 0;
     if (const char* r = std::getenv("KNNG_REFINE_SLOTS")) c->refine_slots = std::max(0, std::atoi(r));
     if (const char* r = std::getenv("KNNG_JOIN_ORDER")) c->join_order_ids = std::strcmp(r, "id") == 0;
-    if (const char* r = std::getenv("KNNG_LEAF")) c->leaf_tc = std::strcmp(r, "fp32") != 0;
+    if (const char* r = std::getenv("KNNG_LEAF")) c->leaf_tc = std::strcmp(r, "tc") == 0;
     if (const char* r = std::getenv("KNNG_REP_LOOP"))
         c->rep_loop = std::strcmp(r, "host") == 0 ? 2 : (std::strcmp(r, "device") == 0 ? 1 : 0);
     c->sms = prop.multiProcessorCount;

@@ -99,10 +99,11 @@ struct Context {
     // The join takes points in the leaf order of the last repetition; true
     // (environment KNNG_JOIN_ORDER=id at creation): in id order.
     bool join_order_ids = false;
-    // FP32 bucket pass: distances only where the tensor-core filter cannot
-    // rule a pair out (k_leaf_tc); false (environment KNNG_LEAF=fp32 at
-    // creation): every pair's distance (k_leaf).  Both give the same sets.
-    bool leaf_tc = true;
+    // FP32 bucket pass: every pair's distance (k_leaf); true (environment
+    // KNNG_LEAF=tc at creation): distances only where the tensor-core filter
+    // cannot rule a pair out (k_leaf_tc).  Both give the same sets; the
+    // filtered pass is slower at 10M points (the set updates dominate).
+    bool leaf_tc = false;
     int64_t refine_pool = -1;
     // Breakdown of the last refinement pass.
     struct RefineRecord {

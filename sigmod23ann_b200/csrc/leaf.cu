@@ -11,8 +11,9 @@
 // memory tiles, then each warp replays its points' 64 offers in column order
 // (set_offer_batch).  Distances are computed for the full b x b matrix (both
 // triangles); each (i, j) and (j, i) evaluation gives the same bits.
-// k_leaf_tc (the default) makes the same offers but computes distances only
-// for the pairs a tensor-core filter cannot rule out (see below).
+// k_leaf_tc makes the same offers but computes distances only for the pairs
+// a tensor-core filter cannot rule out (see below); it is the slower of the
+// two at 10M points, where the sequential set updates dominate.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -537,19 +538,23 @@ __global__ void __launch_bounds__(kLeafThreads, 2)
                 if ((warp & 3) < kBI / kWarp) {
                     const int row = (warp & 3) * kWarp + lane;
                     const int g0 = (warp >> 2) * 16;
-                    float g[16];
-                    tc::tmem_ld16(tmem + (static_cast<uint32_t>((warp & 3) * kWarp) << 16) + g0, g);
-                    tc::tmem_wait_ld();
                     const float na = norm_a[row], ra = rt_a[row], bp = bnd[row];
                     uint32_t m = 0;
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) {
-                        const float nb = norm_b[g0 + u];
-                        const float approx = na + nb - 2.0f * g[u];
-                        const float margin = 0.00390625f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + ra +
-                                             rt_b[g0 + u];
-                        // NaN-safe: a pair is left out only when the bound provably holds.
-                        if (!(approx - margin >= bp)) m |= 1u << u;
+                    for (int hh = 0; hh < 2; ++hh) {  // two loads of 8 columns: fewer live registers
+                        float g[8];
+                        tc::tmem_ld8(tmem + (static_cast<uint32_t>((warp & 3) * kWarp) << 16) + g0 + 8 * hh, g);
+                        tc::tmem_wait_ld();
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            const int j = g0 + 8 * hh + u;
+                            const float nb = norm_b[j];
+                            const float approx = na + nb - 2.0f * g[u];
+                            const float margin =
+                                0.00390625f * (na + nb) + 1.52587890625e-5f * fabsf(approx) + ra + rt_b[j];
+                            // NaN-safe: a pair is left out only when the bound provably holds.
+                            if (!(approx - margin >= bp)) m |= 1u << (8 * hh + u);
+                        }
                     }
                     pass[row * 4 + (warp >> 2)] = static_cast<uint16_t>(m);
                 }

@@ -470,8 +470,8 @@ def test_rep_graph_equals_other_level_loops(knng_lib, monkeypatch, loop):
 @pytest.mark.parametrize("loop", [None, "host"])
 def test_filtered_bucket_pass_equals_plain(knng_lib, monkeypatch, loop):
     """The bucket pass that computes distances only for pairs its tensor-core
-    filter cannot rule out (the default) leaves the same sets, bit for bit, as
-    the pass that computes every pair's distance (KNNG_LEAF=fp32): over
+    filter cannot rule out (KNNG_LEAF=tc) leaves the same sets, bit for bit, as
+    the pass that computes every pair's distance (the default): over
     repetitions whose sets start empty, fill, and then reject most offers,
     with buckets up to 1,024 points, in the graph and in the host level loop."""
     pts = workloads.gaussian_mixture(n=40_000, d=100, clusters=24, sigma=0.2, seed=33)
@@ -494,6 +494,6 @@ def test_filtered_bucket_pass_equals_plain(knng_lib, monkeypatch, loop):
                 out.append(c.sets())
         return out
 
-    filtered, plain = run(None), run("fp32")
+    filtered, plain = run("tc"), run(None)
     for r, (a, b) in enumerate(zip(filtered, plain)):
         assert_sets_equal(a, b, f"rep {r}")
