@@ -116,7 +116,8 @@ void knng_default_params(knng_params* params);
 const char* knng_status_string(knng_status status);
 
 /* Creates a context on CUDA device `device`.  hbm_budget_bytes caps the
- * device memory the context may hold (0 = 90% of the device's memory). */
+ * device memory the context may hold (0 = 90% of the device's memory, or
+ * what is free when the context is created less 1 GiB, whichever is less). */
 knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** out);
 knng_status knng_destroy(knng_context* ctx);
 

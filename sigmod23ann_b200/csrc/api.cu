@@ -703,7 +703,20 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
         c->rep_loop = std::strcmp(r, "host") == 0 ? 2 : (std::strcmp(r, "device") == 0 ? 1 : 0);
     c->sms = prop.multiProcessorCount;
     if (const char* r = std::getenv("KNNG_REFINE_POOL")) c->refine_pool = std::max<long long>(0, std::atoll(r));
-    c->budget = hbm_budget_bytes ? hbm_budget_bytes : static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
+    if (hbm_budget_bytes) {
+        c->budget = hbm_budget_bytes;
+    } else {
+        // 90% of the device, but no more than what is free now (less 1 GiB):
+        // memory other users of the device hold is not this context's.
+        c->budget = static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const uint64_t room = free_b > (1ull << 30) ? free_b - (1ull << 30) : 0;
+            c->budget = std::min<uint64_t>(c->budget, room);
+        } else {
+            cudaGetLastError();
+        }
+    }
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return KNNG_ERR_CUDA;
