@@ -575,10 +575,10 @@ def run_batched(waves: int, device: int = 0) -> dict:
     params = default_params(k=K, max_leaf=MAX_LEAF, max_leaf_odd=0, lloyd_iters=LLOYD_ITERS, reps=REPS,
                             refine=REFINE, seed=SEED)
     dev = f"cuda:{device}"
-    ctx = KnngContext(device)
     total_points, total_ms, recalls, waves_out = 0, 0.0, [], []
-    lib = ctx._lib
     import ctypes
+
+    torch.cuda.empty_cache()  # blocks the caller's earlier work left in torch's cache
 
     for w in range(min(waves, 5)):
         ws = sizes[per_wave[w]]
@@ -587,9 +587,16 @@ def run_batched(waves: int, device: int = 0) -> dict:
         offs[1:] = np.cumsum(ws)
         n = int(offs[-1])
         ids = torch.empty((n, K), dtype=torch.int32, device=dev)
+        # The context is created once the wave's tensors exist, so that its
+        # default budget (bounded by the memory free at creation) leaves them
+        # out.
+        ctx = KnngContext(device)
         st = Stats()
-        ctx._check(lib.knng_build_batch(ctx._h, _ptr(x), n, DIM, DIM * 4, _ptr(offs), len(ws), 1,
-                                        ctypes.byref(params), _ptr(ids), None, ctypes.byref(st)))
+        try:
+            ctx._check(ctx._lib.knng_build_batch(ctx._h, _ptr(x), n, DIM, DIM * 4, _ptr(offs), len(ws), 1,
+                                                 ctypes.byref(params), _ptr(ids), None, ctypes.byref(st)))
+        finally:
+            ctx.close()
         ms = st.ms_total + st.ms_finalize
         total_points += n
         total_ms += ms
@@ -602,7 +609,6 @@ def run_batched(waves: int, device: int = 0) -> dict:
         waves_out.append({"sets": len(ws), "points": n, "ms": ms})
         del x, ids
         torch.cuda.empty_cache()
-    ctx.close()
     return {"sets": int(sum(w["sets"] for w in waves_out)), "points": total_points, "ms": total_ms,
             "points_per_s": total_points / (total_ms / 1000.0), "waves": waves_out,
             "min_recall": float(min(recalls)), "mean_recall": float(np.mean(recalls)),
