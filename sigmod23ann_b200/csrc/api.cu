@@ -134,12 +134,14 @@ size_t scratch_bytes(const Context& c, const char* name) {
 namespace {
 
 void free_points(Context& c) {
+    c.snap_prev_valid = false;
     if (c.points && !c.points_borrowed) dev_free(c, c.points, static_cast<size_t>(c.n) * c.ld * sizeof(float));
     c.points = nullptr;
     c.points_borrowed = false;
 }
 
 void free_sets(Context& c) {
+    c.snap_prev_valid = false;
     const size_t nk = static_cast<size_t>(c.n) * c.k;
     dev_free(c, c.set_dist, nk * sizeof(float));
     dev_free(c, c.set_id, nk * sizeof(uint32_t));
@@ -699,6 +701,7 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
     if (const char* r = std::getenv("KNNG_REFINE_SLOTS")) c->refine_slots = std::max(0, std::atoi(r));
     if (const char* r = std::getenv("KNNG_JOIN_ORDER")) c->join_order_ids = std::strcmp(r, "id") == 0;
     if (const char* r = std::getenv("KNNG_LEAF")) c->leaf_tc = std::strcmp(r, "tc") == 0;
+    if (const char* r = std::getenv("KNNG_REFINE_SKIP")) c->refine_skip_old = std::strcmp(r, "0") != 0;
     if (const char* r = std::getenv("KNNG_REP_LOOP"))
         c->rep_loop = std::strcmp(r, "host") == 0 ? 2 : (std::strcmp(r, "device") == 0 ? 1 : 0);
     c->sms = prop.multiProcessorCount;
@@ -709,6 +712,11 @@ knng_status knng_create(int device, uint64_t hbm_budget_bytes, knng_context** ou
         // 90% of the device, but no more than what is free now (less 1 GiB):
         // memory other users of the device hold is not this context's.
         c->budget = static_cast<uint64_t>(prop.totalGlobalMem * 0.9);
+        // Memory freed to the device's stream-ordered pool (by contexts
+        // destroyed earlier) counts as free: return what the pool keeps unused.
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        cudaGetLastError();
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
             const uint64_t room = free_b > (1ull << 30) ? free_b - (1ull << 30) : 0;
@@ -962,6 +970,7 @@ knng_status knng_set_sets(knng_context* ctx, const float* dist, const uint32_t* 
             if (sizes[i] > c.k) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "set size above k");
             if (sizes[i] == c.k && maxslot[i] >= c.k) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "full set without a max slot");
         }
+        c.snap_prev_valid = false;  // the sets change other than by offers
         const size_t nk = static_cast<size_t>(c.n) * c.k;
         KNNG_CUDA(cudaMemcpyAsync(c.set_dist, dist, nk * sizeof(float), cudaMemcpyHostToDevice, c.stream));
         KNNG_CUDA(cudaMemcpyAsync(c.set_id, ids, nk * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
@@ -1032,6 +1041,7 @@ knng_status knng_load_sets(knng_context* ctx, const char* path) {
             if (size[i] == k && maxslot[i] >= k) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "full set without a max slot");
         }
         knng::alloc_sets(c, k);
+        c.snap_prev_valid = false;  // the sets change other than by offers
         KNNG_CUDA(cudaMemcpyAsync(c.set_dist, dist.data(), nk * sizeof(float), cudaMemcpyHostToDevice, c.stream));
         KNNG_CUDA(cudaMemcpyAsync(c.set_id, ids.data(), nk * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
         KNNG_CUDA(cudaMemcpyAsync(c.set_size, size.data(), c.n * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));

@@ -104,6 +104,13 @@ struct Context {
     // cannot rule a pair out (k_leaf_tc).  Both give the same sets; the
     // filtered pass is slower at 10M points (the set updates dominate).
     bool leaf_tc = false;
+    // A join pass skips the pairs the previous join pass offered (both edges
+    // already in its lists; offering them again changes nothing): the lists
+    // of the last pass are kept while snap_prev_valid.  Any change to the sets
+    // other than offers clears it.  false (environment KNNG_REFINE_SKIP=0 at
+    // creation): every pass offers every pair.
+    bool refine_skip_old = true;
+    bool snap_prev_valid = false;
     int64_t refine_pool = -1;
     // Breakdown of the last refinement pass.
     struct RefineRecord {

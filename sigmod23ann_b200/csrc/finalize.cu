@@ -108,6 +108,7 @@ void launch_finalize(Context& c, uint32_t* d_ids, float* d_dists) {
 }
 
 void launch_reset_sets(Context& c) {
+    c.snap_prev_valid = false;
     if (c.n == 0) return;
     const size_t nk = static_cast<size_t>(c.n) * c.k;
     KNNG_CUDA(cudaMemsetAsync(c.set_dist, 0, nk * sizeof(float), c.stream));

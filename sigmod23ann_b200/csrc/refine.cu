@@ -71,17 +71,47 @@ __host__ __device__ uint32_t pow2_at_least(uint32_t v) {
     return p;
 }
 
+// Words of a point's old-entry mask (one bit per snapshot entry).
+constexpr int kOldWords = kMaxK / kWarp;  // 4
+
+// Each point's sorted list of its set's k slot ids.  With `prev` (the sorted
+// lists of the previous pass) also old[p * kOldWords + i / 32] bit i % 32 =
+// entry i of the new list is in the point's previous list.
 __global__ void __launch_bounds__(kSnapWarps * kWarp) k_snapshot(const uint32_t* __restrict__ set_id, uint32_t n, int K,
-                                                                 uint32_t* __restrict__ snap) {
+                                                                 uint32_t* __restrict__ snap,
+                                                                 const uint32_t* __restrict__ prev,
+                                                                 uint32_t* __restrict__ old) {
     __shared__ unsigned long long keys_s[kSnapWarps][kMaxK];
+    __shared__ uint32_t prev_s[kSnapWarps][kMaxK];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     unsigned long long* keys = keys_s[warp];
+    uint32_t* pl = prev_s[warp];
+    int top = 1;  // largest power of two <= K (branch-free lower bound)
+    while (top * 2 <= K) top *= 2;
     for (uint32_t p = blockIdx.x * kSnapWarps + warp; p < n; p += gridDim.x * kSnapWarps) {
         const size_t base = static_cast<size_t>(p) * K;
         for (int slot = lane; slot < kMaxK; slot += kWarp) keys[slot] = slot < K ? set_id[base + slot] : ~0ull;
+        if (prev)
+            for (int i = lane; i < K; i += kWarp) pl[i] = prev[base + i];
         __syncwarp();
         warp_bitonic_sort(keys, kMaxK, lane);
         for (int i = lane; i < K; i += kWarp) snap[base + i] = static_cast<uint32_t>(keys[i]);
+        if (prev) {
+#pragma unroll
+            for (int w = 0; w < kOldWords; ++w) {
+                const int i = w * kWarp + lane;
+                bool found = false;
+                if (i < K) {
+                    const uint32_t id = static_cast<uint32_t>(keys[i]);
+                    int pos = 0;  // first entry of pl >= id
+                    for (int step = top; step > 0; step >>= 1)
+                        if (pos + step <= K && pl[pos + step - 1] < id) pos += step;
+                    found = pos < K && pl[pos] == id;
+                }
+                const unsigned m = __ballot_sync(kFull, found);
+                if (lane == 0) old[static_cast<size_t>(p) * kOldWords + w] = m;
+            }
+        }
         __syncwarp();
     }
 }
@@ -288,15 +318,27 @@ __global__ void k_rev_count(const uint32_t* __restrict__ snap, uint32_t n, int K
     }
 }
 
+// Bit 31 of a reverse-list entry: the edge p -> q was already in p's list of
+// the previous pass (ids are below 2^31 when the marks are used).
+constexpr uint32_t kOldEdge = 0x80000000u;
+
+// Points are visited in `order` when given (the last repetition's leaf
+// order): neighbouring points fill the same reverse lists close in time, so
+// their 4-byte writes meet in L2 instead of each moving a DRAM sector.
 __global__ void k_rev_fill(const uint32_t* __restrict__ snap, uint32_t n, int K,
                            const unsigned long long* __restrict__ off, uint32_t* __restrict__ cursor,
-                           uint32_t* __restrict__ rev) {
+                           uint32_t* __restrict__ rev, const uint32_t* __restrict__ old,
+                           const uint32_t* __restrict__ order) {
     const int lane = threadIdx.x % kWarp;
-    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < n; p += gridDim.x * blockDim.x / kWarp) {
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp; w < n; w += gridDim.x * blockDim.x / kWarp) {
+        const uint32_t p = order ? order[w] : w;
         const uint32_t* row = snap + static_cast<size_t>(p) * K;
         for (int a = lane; a < K; a += kWarp) {
             const uint32_t q = row[a];
-            if (a == 0 || row[a - 1] != q) rev[off[q] + atomicAdd(&cursor[q], 1u)] = p;
+            if (a == 0 || row[a - 1] != q) {
+                const bool was = old && ((old[static_cast<size_t>(p) * kOldWords + a / kWarp] >> (a % kWarp)) & 1u);
+                rev[off[q] + atomicAdd(&cursor[q], 1u)] = p | (was ? kOldEdge : 0u);
+            }
         }
     }
 }
@@ -564,7 +606,7 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
            uint32_t* __restrict__ surv_count, unsigned long long* __restrict__ surv, uint4* __restrict__ pool,
            uint32_t pool_cap, uint32_t* __restrict__ pool_fill, uint8_t* __restrict__ lost,
            uint32_t* __restrict__ error_flag, unsigned long long* __restrict__ counters,
-           const uint32_t* __restrict__ order, uint32_t* __restrict__ work) {
+           const uint32_t* __restrict__ order, uint32_t* __restrict__ work, const uint32_t* __restrict__ old_marks) {
     using L = JoinLayout<D>;
     extern __shared__ __align__(1024) unsigned char smem[];
     const JoinSmem S = join_smem(D, static_cast<uint32_t>(K));
@@ -589,6 +631,7 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
     __shared__ uint64_t rows_bar, list_bar, mma_bar, arow_bar;
     __shared__ uint32_t tmem_slot;
     __shared__ uint32_t ncols_s;
+    __shared__ uint32_t colold_s[4];  // old columns of the current q (bit per column)
     __shared__ uint32_t pool_cursor;
     __shared__ uint32_t work_s[2];
     const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
@@ -659,6 +702,8 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
                 v[i] = a < K ? __ldg(sq + a) : kNone;
             }
             uint32_t base = 0;
+            if (lane < 4) colold_s[lane] = 0u;
+            __syncwarp();
 #pragma unroll
             for (int i = 0; i < kSlotsPerLane; ++i) {
                 const int a = i * kWarp + lane;
@@ -668,7 +713,13 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
                 if (lane == 0) prev = wrap;
                 const bool keep = a < K && (a == 0 || prev != v[i]);
                 const unsigned m = __ballot_sync(kFull, keep);
-                if (keep) cid[base + __popc(m & lt)] = v[i];
+                if (keep) {
+                    const uint32_t col = base + __popc(m & lt);
+                    cid[col] = v[i];
+                    // Column c of q was already in q's list of the previous pass.
+                    if (old_marks && ((old_marks[static_cast<size_t>(q) * kOldWords + i] >> lane) & 1u))
+                        atomicOr(&colold_s[col / kWarp], 1u << (col % kWarp));
+                }
                 base += __popc(m);
             }
             if (lane == 0) ncols_s = base;
@@ -681,10 +732,13 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
             const uint32_t m = static_cast<uint32_t>(min(static_cast<unsigned long long>(kTile), re - cb));
             const bool with_b = cb == rb;
             if (tid < kTile) {
-                const uint32_t p = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
+                const uint32_t rv = tid < static_cast<int>(m) ? rev[cb + tid] : kNone;
+                // With the marks, bit 31 says the edge p -> q is old.
+                const uint32_t p = rv == kNone ? kNone : (old_marks ? rv & ~kOldEdge : rv);
+                const bool row_old = old_marks && rv != kNone && (rv & kOldEdge);
                 pid[tid] = p;
                 bnd[tid] = p != kNone ? bound[p] : 0.0f;
-                fullrow[tid] = p != kNone && set_size[p] == static_cast<uint32_t>(K) ? 1u : 0u;
+                fullrow[tid] = (p != kNone && set_size[p] == static_cast<uint32_t>(K) ? 1u : 0u) | (row_old ? 2u : 0u);
             }
             __syncthreads();
             JOIN_MARK(2)
@@ -764,6 +818,13 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
                     const int valid_cols = max(0, min(kGroupCols, static_cast<int>(nc) - j0));
                     pass &= valid_cols == kGroupCols ? ~0ull : ((1ull << valid_cols) - 1ull);
                     if (p == kNone) pass = 0;
+                    // A pair whose two edges (p -> q and q -> c) were both in the
+                    // previous pass's lists was offered then: every offer of it
+                    // now is rejected (c is in S(p), or at least as far as a
+                    // bound that has only fallen since).
+                    if (fullrow[row] & 2u)
+                        pass &= ~(static_cast<unsigned long long>(colold_s[2 * group]) |
+                                  static_cast<unsigned long long>(colold_s[2 * group + 1]) << 32);
                     if (p != kNone) {
                         n_pairs += valid_cols;
                         n_pass += __popcll(pass);
@@ -840,7 +901,7 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         if (own[u] >= 0 && pos[u] < K && lst[u][pos[u]] == key[u] &&
-                            (key[u] != lst[u][0] || fullrow[pair_row(own[u])] != 0u)) {
+                            (key[u] != lst[u][0] || (fullrow[pair_row(own[u])] & 1u) != 0u)) {
                             atomicOr(&mem_s[own[u]], 1ull << bit[u]);
                             ++n_member;
                         }
@@ -1194,8 +1255,20 @@ uint64_t run_refine(Context& c) {
     const int K = static_cast<int>(c.k);
     const uint32_t n = c.n;
     uint32_t* snap = static_cast<uint32_t*>(scratch(c, "refine_snap", static_cast<size_t>(n) * K * sizeof(uint32_t)));
+    // The join skips pairs the previous join pass offered (both edges in that
+    // pass's lists): with the previous lists kept, the snapshot marks each
+    // entry that was already there.  Ids must fit 31 bits (the marks ride in
+    // bit 31 of the reverse lists).
+    const size_t old_bytes = static_cast<size_t>(n) * kOldWords * 4;
+    const bool marks = c.refine_mode == 0 && c.refine_skip_old && c.snap_prev_valid && n < (1u << 31) &&
+                       (scratch_bytes(c, "refine_old") >= old_bytes || c.held + old_bytes <= c.budget);
+    uint32_t* prev = marks ? static_cast<uint32_t*>(scratch(c, "refine_snap_prev", static_cast<size_t>(n) * K * 4))
+                           : nullptr;
+    uint32_t* old = marks ? static_cast<uint32_t*>(scratch(c, "refine_old", static_cast<size_t>(n) * kOldWords * 4))
+                          : nullptr;
+    c.snap_prev_valid = false;  // valid again once this pass completes
     const uint32_t sblocks = std::min<uint32_t>((n + kSnapWarps - 1) / kSnapWarps, 148 * 8);
-    k_snapshot<<<sblocks, kSnapWarps * kWarp, 0, c.stream>>>(c.set_id, n, K, snap);
+    k_snapshot<<<sblocks, kSnapWarps * kWarp, 0, c.stream>>>(c.set_id, n, K, snap, prev, old);
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
     if (c.refine_mode == 1) return run_refine_pointwise(c, snap, nullptr, n);
@@ -1215,7 +1288,7 @@ uint64_t run_refine(Context& c) {
     const uint32_t wblocks = std::min<uint32_t>((n + 7) / 8, 148 * 16);
     k_rev_count<<<wblocks, 256, 0, c.stream>>>(snap, n, K, cnt);
     device_scan(c, cnt, n, off);
-    k_rev_fill<<<wblocks, 256, 0, c.stream>>>(snap, n, K, off, cur, rev);
+    k_rev_fill<<<wblocks, 256, 0, c.stream>>>(snap, n, K, off, cur, rev, old, c.join_order_ids ? nullptr : c.indices);
     c.launches += 2;
     KNNG_CUDA(cudaGetLastError());
 
@@ -1259,10 +1332,10 @@ uint64_t run_refine(Context& c) {
         pool_cap = static_cast<uint32_t>(c.refine_pool);
     } else {
         const uint64_t after = avail > static_cast<uint64_t>(n) * slots * 8 ? avail - static_cast<uint64_t>(n) * slots * 8 : 0;
-        // At most 128 records per point on average (the records past the
-        // slots are a small fraction once the slots hold the typical list).
-        const uint64_t want = (static_cast<uint64_t>(n) * 128 + kJoinBlocks - 1) / kJoinBlocks;
-        pool_cap = static_cast<uint32_t>(std::min<uint64_t>({after / 2 / (kJoinBlocks * 16ull), want, 1u << 30}));
+        // Half of what the slots leave: with fewer slots (a smaller budget)
+        // more records go to the pool, and a region that fills sends its
+        // points to the slow per-point pass.
+        pool_cap = static_cast<uint32_t>(std::min<uint64_t>(after / 2 / (kJoinBlocks * 16ull), 1u << 30));
     }
     auto* scount = static_cast<uint32_t*>(scratch(c, "surv_count", static_cast<size_t>(n) * sizeof(uint32_t)));
     auto* ocount = static_cast<uint32_t*>(scratch(c, "surv_excess", static_cast<size_t>(n) * sizeof(uint32_t)));
@@ -1303,7 +1376,7 @@ uint64_t run_refine(Context& c) {
     KNNG_DISPATCH_D(c.d, {
         k_join<D><<<kJoinBlocks, kJoinThreads, join_bytes, c.stream>>>(snap, off, rev, c.points, c.ld, c.set_bound, c.set_size, K,
                                                             n, slots, scount, direct, pool, pool_cap, pool_fill, lost,
-                                                            err, jc, order, work);
+                                                            err, jc, order, work, old);
     });
     ++c.launches;
     ++rec.join_launches;
@@ -1409,6 +1482,15 @@ uint64_t run_refine(Context& c) {
     rec.overflow = total;
     rec.lost = lost_points;
     c.last_refine = rec;
+    // This pass offered every pair of its lists: keep them for the next one
+    // (when the budget has room for them; else the next pass skips nothing).
+    const size_t snap_bytes = static_cast<size_t>(n) * K * 4;
+    if (c.refine_skip_old && n < (1u << 31) &&
+        (scratch_bytes(c, "refine_snap_prev") >= snap_bytes || c.held + snap_bytes + old_bytes <= c.budget)) {
+        uint32_t* keep = static_cast<uint32_t*>(scratch(c, "refine_snap_prev", static_cast<size_t>(n) * K * 4));
+        KNNG_CUDA(cudaMemcpyAsync(keep, snap, static_cast<size_t>(n) * K * 4, cudaMemcpyDeviceToDevice, c.stream));
+        c.snap_prev_valid = true;
+    }
     return changed;
 }
 
@@ -1534,7 +1616,7 @@ extern "C" knng_status knng_refine_pointwise_noalloc(const float* d_points, uint
         return KNNG_ERR_CUDA;
     }
     const uint32_t sblocks = std::min<uint32_t>((n + kSnapWarps - 1) / kSnapWarps, 148 * 8);
-    k_snapshot<<<sblocks, kSnapWarps * kWarp, 0, s>>>(d_ids, n, K, d_snapshot);
+    k_snapshot<<<sblocks, kSnapWarps * kWarp, 0, s>>>(d_ids, n, K, d_snapshot, nullptr, nullptr);
     try {
         KNNG_DISPATCH_D(d, {
             k_refine<D><<<blocks, kRefWarps * kWarp, 0, s>>>(d_snapshot, d_points, static_cast<int>(d), d_dist,

@@ -497,3 +497,54 @@ def test_filtered_bucket_pass_equals_plain(knng_lib, monkeypatch, loop):
     filtered, plain = run("tc"), run(None)
     for r, (a, b) in enumerate(zip(filtered, plain)):
         assert_sets_equal(a, b, f"rep {r}")
+
+
+def test_later_passes_skip_old_pairs_and_match_oracle(oracle_lib, monkeypatch):
+    """A neighbour-of-neighbour pass after the first leaves out the pairs whose
+    two edges were both in the previous pass's lists (offering them again
+    changes nothing).  Three passes after two repetitions, a pass between
+    repetitions, and sets whose lists change a lot between passes: every
+    pass's set state equals the oracle's (which offers every pair) and the
+    build with the skip switched off (KNNG_REFINE_SKIP=0), bit for bit."""
+    from sigmod23ann_b200.api import Stats
+
+    pts = workloads.gaussian_mixture(n=12_000, d=100, clusters=24, sigma=0.2, seed=44)
+
+    def run(skip):
+        if skip:
+            monkeypatch.delenv("KNNG_REFINE_SKIP", raising=False)
+        else:
+            monkeypatch.setenv("KNNG_REFINE_SKIP", "0")
+        out, stats = [], []
+        with KnngContext(0) as c:
+            c.load_points(pts)
+            c.reset_sets(100)
+            for step in ["rep", "rep", "pass", "rep", "pass", "pass", "pass"]:
+                if step == "rep":
+                    r = sum(1 for s in out if s[0] == "rep")
+                    c.run_rep(257 if r % 2 == 0 else 400, 2, 3000, seed=77, rep_index=r)
+                    out.append(("rep", c.sets()))
+                else:
+                    st = Stats()
+                    c.refine(st)
+                    out.append(("pass", c.sets()))
+                    stats.append(int(st.refine_filter_pass))
+        return out, stats
+
+    with_skip, pass_with = run(True)
+    without, pass_without = run(False)
+    for i, ((kind, a), (_, b)) in enumerate(zip(with_skip, without)):
+        assert_sets_equal(a, b, f"step {i} ({kind})")
+    # The first pass skips nothing; the later ones leave pairs out.
+    assert pass_with[0] == pass_without[0]
+    assert all(w < wo for w, wo in zip(pass_with[1:], pass_without[1:])), (pass_with, pass_without)
+    # And the oracle (every pair offered, counter RNG) agrees after each pass.
+    o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=77)
+    reps = 0
+    for i, (kind, sets) in enumerate(with_skip):
+        if kind == "rep":
+            o.rep(2, 257 if reps % 2 == 0 else 400, reps)
+            reps += 1
+        else:
+            o.refine()
+        assert_sets_equal(sets, o.sets(), f"oracle step {i} ({kind})")
