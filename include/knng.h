@@ -203,6 +203,19 @@ knng_status knng_process_leaves(knng_context* ctx, uint32_t count, const uint32_
 knng_status knng_run_rep(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold,
                          uint64_t seed, uint32_t rep_index, knng_stats* stats);
 
+/* Bucket-pass autotuner (no counterpart in the reference; the reference has a
+ * single CPU loop, src/KnnSets.hpp:131-160).  Times the FP32 bucket-pass
+ * variants on one repetition of the context's own points and current sets
+ * (max_leaf, lloyd_iters, small_threshold, seed as knng_run_rep, rep_index 0),
+ * restoring the sets before each trial and after the last: 0 = every pair's
+ * distance, 2 persistent CTAs per SM (the default); 1 = the same, 1 CTA per
+ * SM; 2 = distances only for pairs a tensor-core filter cannot rule out, 2
+ * CTAs per SM; 3 = the same, 1 CTA per SM.  All four give the same sets.  The
+ * fastest is kept for the context's later repetitions.  out_ms[4] (optional):
+ * each variant's bucket-pass ms; *out_choice (optional): the variant kept. */
+knng_status knng_tune_buckets(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold,
+                              uint64_t seed, double* out_ms, uint32_t* out_choice);
+
 /* Leaf ranges of the last knng_run_rep, in position order. */
 knng_status knng_get_leaves(knng_context* ctx, uint32_t capacity, uint32_t* starts, uint32_t* ends,
                             uint32_t* out_count);

@@ -33,7 +33,7 @@ PRECISION_BF16_RERANK = 1
 EXPORTED = [
     "knng_default_params", "knng_status_string", "knng_create", "knng_destroy", "knng_last_error", "knng_build",
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
-    "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_get_leaves", "knng_refine",
+    "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_tune_buckets", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
     "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_debug_set_wait_limit", "knng_refine_pointwise_noalloc",
     "knng_build_batch",
@@ -111,6 +111,8 @@ def load_library(path: str = LIB_PATH):
         "knng_lloyd": (c_int, [P, c_uint32, P, P, P, P, P, P, c_uint32, P, P, P]),
         "knng_process_leaves": (c_int, [P, c_uint32, P, P]),
         "knng_run_rep": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, c_uint32, POINTER(Stats)]),
+        "knng_tune_buckets": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, POINTER(ctypes.c_double),
+                                      POINTER(c_uint32)]),
         "knng_get_leaves": (c_int, [P, c_uint32, P, P, P]),
         "knng_refine": (c_int, [P, P, POINTER(Stats)]),
         "knng_get_indices": (c_int, [P, P]),
@@ -348,6 +350,17 @@ class KnngContext:
         self._check(self._lib.knng_run_rep(self._h, max_leaf, lloyd_iters, small_threshold, seed, rep_index,
                                            ctypes.byref(st)))
         return st
+
+    def tune_buckets(self, max_leaf: int, lloyd_iters: int, small_threshold: int = 3000,
+                     seed: int = 12345) -> tuple[list[float], int]:
+        """knng_tune_buckets: bucket-pass ms of the four variants (every pair /
+        tensor-core filtered, x 2 / 1 CTAs per SM) on one repetition of the
+        current points and sets (restored afterwards), and the variant kept."""
+        ms = (ctypes.c_double * 4)()
+        choice = c_uint32()
+        self._check(self._lib.knng_tune_buckets(self._h, max_leaf, lloyd_iters, small_threshold, seed, ms,
+                                                ctypes.byref(choice)))
+        return [float(v) for v in ms], int(choice.value)
 
     def leaves(self):
         cnt = c_uint32()

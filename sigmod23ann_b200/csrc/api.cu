@@ -903,6 +903,61 @@ knng_status knng_run_rep(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_it
     });
 }
 
+knng_status knng_tune_buckets(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold,
+                              uint64_t seed, double* out_ms, uint32_t* out_choice) {
+    return knng::guarded(ctx, [&](Context& c) {
+        if (max_leaf < 2 || max_leaf > 4097) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be in [2, 4097]");
+        knng::require_sets(c);
+        // The sets before the trials, restored before each trial and after.
+        const size_t nk = static_cast<size_t>(c.n) * c.k;
+        const size_t sizes[5] = {nk * 4, nk * 4, static_cast<size_t>(c.n) * 4, static_cast<size_t>(c.n) * 4,
+                                 static_cast<size_t>(c.n) * 4};
+        void* live[5] = {c.set_dist, c.set_id, c.set_size, c.set_maxslot, c.set_bound};
+        void* saved[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+        const bool tc0 = c.leaf_tc;
+        const uint32_t ctas0 = c.leaf_ctas;
+        auto restore = [&]() {
+            for (int i = 0; i < 5; ++i)
+                KNNG_CUDA(cudaMemcpyAsync(live[i], saved[i], sizes[i], cudaMemcpyDeviceToDevice, c.stream));
+        };
+        double ms[4] = {0, 0, 0, 0};
+        try {
+            for (int i = 0; i < 5; ++i) {
+                saved[i] = knng::dev_alloc(c, sizes[i]);
+                KNNG_CUDA(cudaMemcpyAsync(saved[i], live[i], sizes[i], cudaMemcpyDeviceToDevice, c.stream));
+            }
+            // Variants: bucket kernel (every pair / tensor-core filtered) x
+            // persistent CTAs per SM (2 / 1); the same repetition each time.
+            for (uint32_t v = 0; v < 4; ++v) {
+                restore();
+                c.leaf_tc = v >= 2;
+                c.leaf_ctas = v % 2 == 0 ? 2u : 1u;
+                knng::RepStats st;
+                knng::run_rep(c, max_leaf, lloyd_iters, small_threshold, seed, 0, st, nullptr);
+                ms[v] = st.ms_leaf;
+            }
+            restore();
+            KNNG_CUDA(cudaStreamSynchronize(c.stream));
+        } catch (...) {
+            c.leaf_tc = tc0;
+            c.leaf_ctas = ctas0;
+            for (int i = 0; i < 5; ++i) knng::dev_free(c, saved[i], sizes[i]);
+            c.snap_prev_valid = false;
+            throw;
+        }
+        for (int i = 0; i < 5; ++i) knng::dev_free(c, saved[i], sizes[i]);
+        uint32_t best = 0;
+        for (uint32_t v = 1; v < 4; ++v)
+            if (ms[v] < ms[best]) best = v;
+        c.leaf_tc = best >= 2;
+        c.leaf_ctas = best % 2 == 0 ? 2u : 1u;
+        c.snap_prev_valid = false;
+        if (out_ms)
+            for (int v = 0; v < 4; ++v) out_ms[v] = ms[v];
+        if (out_choice) *out_choice = best;
+    });
+}
+
 knng_status knng_get_leaves(knng_context* ctx, uint32_t capacity, uint32_t* starts, uint32_t* ends,
                             uint32_t* out_count) {
     return knng::guarded(ctx, [&](Context& c) {

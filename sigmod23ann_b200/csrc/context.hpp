@@ -104,6 +104,9 @@ struct Context {
     // cannot rule a pair out (k_leaf_tc).  Both give the same sets; the
     // filtered pass is slower at 10M points (the set updates dominate).
     bool leaf_tc = false;
+    // Persistent CTAs per SM of the FP32 bucket pass over the device leaf
+    // list (2 or 1); knng_tune_buckets may change this and leaf_tc.
+    uint32_t leaf_ctas = 2;
     // A join pass skips the pairs the previous join pass offered (both edges
     // already in its lists; offering them again changes nothing): the lists
     // of the last pass are kept while snap_prev_valid.  Any change to the sets

@@ -703,11 +703,10 @@ void launch_leaves_list(Context& c, const uint32_t* d_starts, const uint32_t* d_
             if (smem > 227 * 1024) fail(KNNG_ERR_INVALID_ARGUMENT, "bucket too large for the bucket kernel");
             auto kern = k_leaf_tc<D>;
             allow_max_smem(c, kern);
-            // Persistent: two CTAs per SM take the buckets from the work counter.
-            kern<<<2 * c.sms, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld,
-                                                              c.set_dist, c.set_id, c.set_size, c.set_maxslot,
-                                                              c.set_bound, static_cast<int>(c.k), d_count, d_work,
-                                                              d_error);
+            // Persistent: leaf_ctas CTAs per SM take the buckets from the work counter.
+            kern<<<c.leaf_ctas * c.sms, kLeafThreads, smem, c.stream>>>(
+                d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist, c.set_id, c.set_size, c.set_maxslot,
+                c.set_bound, static_cast<int>(c.k), d_count, d_work, d_error);
         });
         ++c.launches;
         KNNG_CUDA(cudaGetLastError());
@@ -721,8 +720,8 @@ void launch_leaves_list(Context& c, const uint32_t* d_starts, const uint32_t* d_
         auto kern = k_leaf<D>;
         allow_max_smem(c, kern);
         const int sms = c.sms;
-        // Persistent: two CTAs per SM take the buckets from the work counter.
-        kern<<<2 * sms, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
+        // Persistent: leaf_ctas CTAs per SM take the buckets from the work counter.
+        kern<<<c.leaf_ctas * sms, kLeafThreads, smem, c.stream>>>(d_starts, d_ends, c.indices, c.points, c.ld, c.set_dist,
                                                         c.set_id, c.set_size, c.set_maxslot, c.set_bound,
                                                         static_cast<int>(c.k), d_count, d_work);
     });

@@ -1033,6 +1033,7 @@ struct DevRep {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     struct Graph {
         uint32_t max_leaf, lloyd_iters, precision;
+        uint32_t leaf_variant;  // bucket kernel and CTAs per SM baked into the graph
         const void* ptrs[8];
         cudaGraph_t graph;
         cudaGraphExec_t exec;
@@ -1267,11 +1268,12 @@ void enqueue_buckets(Context& c, DevRep& r, uint32_t max_leaf, uint32_t precisio
 DevRep::Graph& rep_graph(Context& c, DevRep& r, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t precision) {
     const void* ptrs[8] = {c.points, c.indices, c.indices_tmp, c.set_dist, c.set_id, c.set_size, c.set_bound,
                            reinterpret_cast<const void*>(static_cast<uintptr_t>(c.k))};
+    const uint32_t variant = (c.leaf_tc ? 4u : 0u) | c.leaf_ctas;
     for (auto& g : r.graphs)
         if (g.max_leaf == max_leaf && g.lloyd_iters == lloyd_iters && g.precision == precision &&
-            std::equal(ptrs, ptrs + 8, g.ptrs))
+            g.leaf_variant == variant && std::equal(ptrs, ptrs + 8, g.ptrs))
             return g;
-    DevRep::Graph g{max_leaf, lloyd_iters, precision, {}, nullptr, nullptr};
+    DevRep::Graph g{max_leaf, lloyd_iters, precision, variant, {}, nullptr, nullptr};
     std::copy(ptrs, ptrs + 8, g.ptrs);
     const uint64_t launches0 = c.launches;
     // Attributes first: nothing but stream work may happen during the capture.

@@ -548,3 +548,33 @@ def test_later_passes_skip_old_pairs_and_match_oracle(oracle_lib, monkeypatch):
         else:
             o.refine()
         assert_sets_equal(sets, o.sets(), f"oracle step {i} ({kind})")
+
+
+def test_bucket_tuner_restores_sets_and_changes_no_result(knng_lib):
+    """knng_tune_buckets times the four bucket-pass variants on a repetition of
+    the context's points and sets and keeps the fastest: the sets afterwards
+    are the ones before, and the next repetitions and a pass give the same
+    sets, bit for bit, as a context that was never tuned."""
+    pts = workloads.gaussian_mixture(n=30_000, d=100, clusters=16, sigma=0.2, seed=55)
+
+    def run(tune):
+        with KnngContext(0) as c:
+            c.load_points(pts)
+            c.reset_sets(100)
+            c.run_rep(1025, 2, 3000, seed=8, rep_index=0)
+            tuned = None
+            if tune:
+                before = c.sets()
+                ms, choice = c.tune_buckets(1025, 2, 3000, seed=8)
+                assert all(m > 0 for m in ms) and 0 <= choice < 4
+                assert choice == int(np.argmin(ms))
+                assert_sets_equal(c.sets(), before, "after tuning")
+                tuned = choice
+            for r in (1, 2):
+                c.run_rep(257 if r == 1 else 1025, 2, 3000, seed=8, rep_index=r)
+            c.refine()
+            return c.sets(), tuned
+
+    tuned_sets, choice = run(True)
+    plain_sets, _ = run(False)
+    assert_sets_equal(tuned_sets, plain_sets, f"tuned (variant {choice}) vs untuned")
