@@ -66,6 +66,8 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work per reference sample")
     ap.add_argument("--serving-requests", type=int, default=200,
                     help="requests of the serving stream measured beside the build")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="skip the bucket-pass autotuner before the timed builds")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="skip the precision, batched and serving figures of the default line")
     ap.add_argument("--serving", action="store_true", help="measure only the serving stream")
@@ -637,6 +639,13 @@ def run_ours(args):
     ctx = KnngContext(local)
     for _ in range(args.warmup):
         ctx.build_device(x.data_ptr(), n, DIM, ids.data_ptr(), None, params)
+    # The bucket-pass autotuner, on the warm-up build's points and sets (they
+    # are restored): the timed builds use the variant it keeps.
+    tuning = None
+    if args.tune and not args.bf16 and args.warmup > 0:
+        tms, choice = ctx.tune_buckets(max_leaf, LLOYD_ITERS, 3000, SEED)
+        names = ["every pair x2", "every pair x1", "tc filter x2", "tc filter x1"]
+        tuning = {"ms": [round(v, 1) for v in tms], "kept": names[choice]}
     torch.cuda.synchronize()
     dist_barrier(world)
     clocks = ClockSampler(local)
@@ -751,7 +760,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(n, args.reps, args.refine, max_leaf, args.bf16, world),
             "clocks": {k: clock[k] for k in ("sm_mhz", "sm_max_mhz", "reasons") if k in clock},
-            "gpu_launches": launches, "roofline": roofline, "e2e": e2e,
+            "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "bucket_tuning": tuning,
             "stages_ms_last_step": stages,
         }
         if adaptive is not None:
