@@ -993,12 +993,13 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
 
 // Replays one point's survivors (buf[0..S), padded to P2 with ~0 and
 // sorted here) through the sequential set update in ascending id order.
-__device__ __forceinline__ uint32_t replay_sorted(unsigned long long* buf, uint32_t S, uint32_t P2, uint32_t p, int K,
-                                                  float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
-                                                  uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
-                                                  float* __restrict__ set_bound, int lane) {
-    __syncwarp();
-    warp_bitonic_sort(buf, P2, lane);
+// Replays a point's survivors buf[0..S), sorted by candidate id, through the
+// sequential set update (a candidate repeated through several shared
+// neighbours is offered once); returns 1 if the set changed.  One warp.
+__device__ __forceinline__ uint32_t replay_keys(const unsigned long long* buf, uint32_t S, uint32_t p, int K,
+                                                float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
+                                                uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
+                                                float* __restrict__ set_bound, int lane) {
     WarpSet s;
     set_load(s, set_dist, set_id, set_size, set_maxslot, set_bound, p, K, lane);
     uint32_t changed = 0;
@@ -1012,6 +1013,16 @@ __device__ __forceinline__ uint32_t replay_sorted(unsigned long long* buf, uint3
         changed += set_offer_batch(s, cid, d, valid, K, lane);
     }
     set_store(s, set_dist, set_id, set_size, set_maxslot, set_bound, p, K, lane);
+    return changed;
+}
+
+__device__ __forceinline__ uint32_t replay_sorted(unsigned long long* buf, uint32_t S, uint32_t P2, uint32_t p, int K,
+                                                  float* __restrict__ set_dist, uint32_t* __restrict__ set_id,
+                                                  uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
+                                                  float* __restrict__ set_bound, int lane) {
+    __syncwarp();
+    warp_bitonic_sort(buf, P2, lane);
+    const uint32_t changed = replay_keys(buf, S, p, K, set_dist, set_id, set_size, set_maxslot, set_bound, lane);
     __syncwarp();
     return changed;
 }
@@ -1056,7 +1067,61 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
     }
 }
 
-// Queued points with more than kApplyCap survivors: sorted in a per-warp
+constexpr int kBigCtaThreads = 256;
+constexpr uint32_t kBigSmemKeys = 8192;  // survivor keys one CTA sorts in shared memory (64 KB)
+
+// Queued points with more than kApplyCap survivors and at most kBigSmemKeys:
+// one CTA per point gathers the list into shared memory, sorts it with every
+// thread (bitonic), and its first warp replays it.  Longer lists are queued
+// on `rest` for k_apply_big.
+__global__ void __launch_bounds__(kBigCtaThreads)
+    k_apply_big_cta(const uint32_t* __restrict__ big, const uint32_t* __restrict__ big_n, int K,
+                    const uint32_t* __restrict__ surv_count, uint32_t slots,
+                    const unsigned long long* __restrict__ surv, const unsigned long long* __restrict__ ovf_off,
+                    const unsigned long long* __restrict__ ovf, float* __restrict__ set_dist,
+                    uint32_t* __restrict__ set_id, uint32_t* __restrict__ set_size, uint32_t* __restrict__ set_maxslot,
+                    float* __restrict__ set_bound, uint32_t* __restrict__ changed_count, uint32_t* __restrict__ rest,
+                    uint32_t* __restrict__ rest_n) {
+    extern __shared__ unsigned long long keys[];  // kBigSmemKeys
+    const int tid = threadIdx.x, lane = tid % kWarp, warp = tid / kWarp;
+    const uint32_t total = *big_n;
+    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+        const uint32_t p = big[w];
+        const uint32_t S = surv_count[p];
+        const uint32_t P2 = pow2_at_least(S);
+        if (P2 > kBigSmemKeys) {  // uniform over the CTA
+            if (tid == 0) rest[atomicAdd(rest_n, 1u)] = p;
+            continue;
+        }
+        const unsigned long long* direct = surv + static_cast<size_t>(p) * slots;
+        const unsigned long long* more = S > slots ? ovf + ovf_off[p] : nullptr;
+        for (uint32_t t = tid; t < P2; t += kBigCtaThreads)
+            keys[t] = t < S ? (t < slots ? direct[t] : more[t - slots]) : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P2; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = tid; t < P2 / 2; t += kBigCtaThreads) {
+                    const uint32_t i = 2 * j * (t / j) + (t % j);
+                    const uint32_t partner = i + j;
+                    const bool up = (i & k) == 0;
+                    const unsigned long long a = keys[i], b = keys[partner];
+                    if ((a > b) == up) {
+                        keys[i] = b;
+                        keys[partner] = a;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (warp == 0) {
+            const uint32_t ch = replay_keys(keys, S, p, K, set_dist, set_id, set_size, set_maxslot, set_bound, lane);
+            if (ch && lane == 0) atomicAdd(changed_count, 1u);
+        }
+        __syncthreads();  // the keys are read before the next point's gather
+    }
+}
+
+// Queued points with more than kBigSmemKeys survivors: sorted in a per-warp
 // global scratch region of `cap` (a power of two >= the largest list) entries.
 __global__ void __launch_bounds__(kRefWarps * kWarp)
     k_apply_big(const uint32_t* __restrict__ big, const uint32_t* __restrict__ big_n, int K,
@@ -1414,7 +1479,22 @@ uint64_t run_refine(Context& c) {
                                                          counters, counters + 1);
     ++c.launches;
     KNNG_CUDA(cudaGetLastError());
+    uint32_t* rest = nullptr;
     if (max_count > static_cast<uint32_t>(kApplyCap)) {
+        // Lists of up to kBigSmemKeys: one CTA each, sorted in shared memory.
+        // counters[2] (the largest count, already read) becomes the count of
+        // the longer lists queued for the per-warp global sort below.
+        rest = static_cast<uint32_t*>(scratch(c, "apply_rest", static_cast<size_t>(n) * sizeof(uint32_t)));
+        KNNG_CUDA(cudaMemsetAsync(counters + 2, 0, sizeof(uint32_t), c.stream));
+        const size_t big_smem = kBigSmemKeys * sizeof(unsigned long long);
+        allow_max_smem(c, k_apply_big_cta);
+        k_apply_big_cta<<<2 * sms, kBigCtaThreads, big_smem, c.stream>>>(
+            big, counters, K, scount, slots, direct, soff, ovf, c.set_dist, c.set_id, c.set_size, c.set_maxslot,
+            c.set_bound, counters + 1, rest, counters + 2);
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
+    }
+    if (max_count > kBigSmemKeys) {
         // Each block's warps sort in big_cap keys of global scratch, which
         // stays within half of L2 (the sorts make many passes over it): one
         // block per SM at most, fewer (a longer grid stride) for large lists
@@ -1427,7 +1507,7 @@ uint64_t run_refine(Context& c) {
             1, std::min<uint64_t>({static_cast<uint64_t>(sms), room / per_block, l2_half / per_block})));
         auto* big_keys = static_cast<unsigned long long*>(
             scratch(c, "apply_big_keys", static_cast<size_t>(big_blocks) * per_block));
-        k_apply_big<<<big_blocks, kRefWarps * kWarp, 0, c.stream>>>(big, counters, K, scount, slots, direct, soff, ovf,
+        k_apply_big<<<big_blocks, kRefWarps * kWarp, 0, c.stream>>>(rest, counters + 2, K, scount, slots, direct, soff, ovf,
                                                                     big_keys, big_cap, c.set_dist, c.set_id,
                                                                     c.set_size, c.set_maxslot, c.set_bound,
                                                                     counters + 1);

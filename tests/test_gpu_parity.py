@@ -578,3 +578,36 @@ def test_bucket_tuner_restores_sets_and_changes_no_result(knng_lib):
     tuned_sets, choice = run(True)
     plain_sets, _ = run(False)
     assert_sets_equal(tuned_sets, plain_sets, f"tuned (variant {choice}) vs untuned")
+
+
+def test_refine_long_survivor_lists_equal_pointwise(knng_lib, monkeypatch):
+    """k = 128 and three repetitions of buckets under 43 points: each set holds
+    up to 126 ids (not full, so its bound is still FLT_MAX) from three
+    different buckets, and every neighbour brings about 84 candidates of its
+    own, so every pair survives: thousands of records per point, many past
+    8,192.  The join's replay sorts lists of 1,025-8,192 records in shared
+    memory (one CTA each) and longer ones in global scratch; both must leave
+    the sets the one-warp-per-point pass leaves."""
+    from sigmod23ann_b200.api import Stats
+
+    pts = workloads.gaussian_mixture(n=20_000, d=100, clusters=16, sigma=0.2, seed=71)
+    with KnngContext(0) as a:
+        a.load_points(pts)
+        a.reset_sets(128)
+        for r in range(3):
+            a.run_rep(43, 2, 3000, seed=3, rep_index=r)
+        s0 = a.sets()
+        st = Stats()
+        a.refine(st)
+        joined = a.sets()
+    assert (s0["size"] < 128).mean() > 0.9
+    # Records per point well past the per-warp sort's 1,024 on average.
+    assert st.refine_emits > 2_000 * len(pts), st.refine_emits
+    monkeypatch.setenv("KNNG_REFINE", "pointwise")
+    with KnngContext(0) as b:
+        b.load_points(pts)
+        b.reset_sets(128)
+        b.set_sets(s0)
+        b.refine()
+        pointwise = b.sets()
+    assert_sets_equal(joined, pointwise, "join vs pointwise, long lists")
