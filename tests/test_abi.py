@@ -161,3 +161,13 @@ def test_null_handles_are_refused(knng_lib):
 def test_set_state_entry_points_refuse_null(knng_lib):
     assert knng_lib.knng_save_sets(None, b"/nonexistent") == 1
     assert knng_lib.knng_load_sets(None, b"/nonexistent") == 1
+
+
+def test_schedule_and_tuning_entry_points_refuse_null(knng_lib):
+    """The adaptive schedule, the bucket-pass autotuner and the wait-limit
+    diagnostic answer KNNG_ERR_INVALID_ARGUMENT for a null context."""
+    ms = (ctypes.c_double * 4)()
+    choice = ctypes.c_uint32()
+    assert knng_lib.knng_tune_buckets(None, 1025, 2, 3000, 1, ms, ctypes.byref(choice)) == 1
+    assert knng_lib.knng_debug_set_wait_limit(None, 0) == 1
+    assert knng_lib.knng_build_adaptive(None, None, 10, 100, 400, None, 0.9, 10, None, None, None) == 1
