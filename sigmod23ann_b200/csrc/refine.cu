@@ -208,21 +208,31 @@ __global__ void __launch_bounds__(kRefWarps * kWarp)
 // pair that goes through q.  Each block reads |R(q)| + |S(q)| rows instead of
 // one row per (p, candidate), and its dot products run on the tensor cores:
 //
-//   1. k_rev_count / scan / k_rev_fill   R(q) as a CSR (counting sort)
-//   2. k_join     per q: S(q) rows and 128-point chunks of R(q) rows, bulk-
-//                 copied into shared memory once, centred on q into FP16
-//                 tiles; one tcgen05 128 x 128 tile gives approximate squared
-//                 distances with a proven error bound, so a pair is dropped
-//                 only when its exact distance is certainly >= bound(p).
+//   1. k_rev_count / scan / k_rev_fill   R(q) as a CSR (counting sort; the
+//                 points visited in leaf order so that the scattered writes
+//                 meet in L2).  After a first pass, an entry whose edge p -> q
+//                 was already in p's previous list carries bit 31.
+//   2. k_join     two persistent CTAs per SM take the points q in leaf order:
+//                 S(q)'s rows bulk-copied into shared memory, the rows of a
+//                 128-point chunk of R(q) converted straight from global
+//                 memory, both centred on q into FP16 tiles; one tcgen05
+//                 128 x N tile gives approximate squared distances with a
+//                 proven error bound, so a pair is dropped only when its exact
+//                 distance is certainly >= bound(p), or (after a first pass)
+//                 when both its edges are old (the previous pass offered it).
 //                 Survivors are checked against S(p) (binary search in shared
 //                 memory: members are always rejected by the set update), get
 //                 the exact FP32 distance in the reference's order from the
-//                 staged rows, and when it beats bound(p) are appended to p's
-//                 survivor slots.
-//   3. k_apply    per p: survivors sorted by id, duplicates dropped, replayed
-//                 through the sequential set update in ascending id order --
-//                 the same offers, in the same order, as the per-point pass.
-//   Points whose survivors overflow their slots are redone by k_refine.
+//                 chunk's rows staged in the freed tile space, and when it
+//                 beats bound(p) are appended to p's survivor slots or the
+//                 CTA's pool region.
+//   3. k_apply    per p: survivors sorted by id (one warp up to 1,024,
+//                 k_apply_big_cta up to 8,192, k_apply_big beyond),
+//                 duplicates dropped, replayed through the sequential set
+//                 update in ascending id order -- the same offers, in the same
+//                 order, as the per-point pass.
+//   Points whose records did not fit their CTA's pool region are redone by
+//   k_refine.
 
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
