@@ -945,6 +945,26 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
             ph_arow ^= 1u;
             JOIN_MARK(10)
             {
+                // A survivor's slot comes from an atomic on its point's count,
+                // whose result the record's store needs: the atomic of the
+                // previous survivor is issued before the next distance, so
+                // its round trip overlaps that arithmetic.
+                bool held = false;
+                uint32_t h_p = 0, h_c = 0;
+                float h_d = 0.0f;
+                auto store = [&](uint32_t slot) {
+                    if (slot < slots) {
+                        surv[static_cast<size_t>(h_p) * slots + slot] =
+                            (static_cast<unsigned long long>(h_c) << 32) | __float_as_uint(h_d);
+                    } else {
+                        const uint32_t e = atomicAdd(&pool_cursor, 1u);
+                        if (e < pool_cap)
+                            pool[static_cast<size_t>(blockIdx.x) * pool_cap + e] =
+                                make_uint4(h_p, h_c, __float_as_uint(h_d), 0u);
+                        else
+                            lost[h_p] = 1;
+                    }
+                };
                 PairCursor cur = pair_share(pref, todo_s);
 #pragma unroll 1
                 while (cur.lo < cur.hi) {
@@ -956,24 +976,19 @@ __global__ void __launch_bounds__(kJoinThreads, kJoinPerSm)
                     const uint32_t c = cid[j];
                     if (c == pp) continue;
                     ++n_exact;
+                    const uint32_t slot = held ? atomicAdd(&surv_count[h_p], 1u) : 0u;
                     const float d = canonical_distance4_lean<D>(reinterpret_cast<const float4*>(rows_b + j * D),
                                                                 reinterpret_cast<const float4*>(arows + prow * D));
-                    if (d < bnd[prow]) {
+                    if (held) store(slot);
+                    held = d < bnd[prow];
+                    if (held) {
                         ++n_emit;
-                        const uint32_t s = atomicAdd(&surv_count[pp], 1u);
-                        if (s < slots) {
-                            surv[static_cast<size_t>(pp) * slots + s] =
-                                (static_cast<unsigned long long>(c) << 32) | __float_as_uint(d);
-                        } else {
-                            const uint32_t e = atomicAdd(&pool_cursor, 1u);
-                            if (e < pool_cap)
-                                pool[static_cast<size_t>(blockIdx.x) * pool_cap + e] =
-                                    make_uint4(pp, c, __float_as_uint(d), 0u);
-                            else
-                                lost[pp] = 1;
-                        }
+                        h_p = pp;
+                        h_c = c;
+                        h_d = d;
                     }
                 }
+                if (held) store(atomicAdd(&surv_count[h_p], 1u));
             }
             // Every thread is done with the rows, lists and TMEM before the
             // next chunk's copies and MMA.
