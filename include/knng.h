@@ -203,6 +203,26 @@ knng_status knng_process_leaves(knng_context* ctx, uint32_t count, const uint32_
 knng_status knng_run_rep(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold,
                          uint64_t seed, uint32_t rep_index, knng_stats* stats);
 
+/* Random-rotation KD splitter, the reference's alternative solution
+ * (SolutionRandomKD, src/SolutionRandomKD.hpp:258-375, disabled at
+ * src/main.cpp:58), behind the same side test, partition and bucket pass:
+ * one repetition -- indices = iota, new_dims (1..32) rotated dimensions from
+ * the rotation of knng_kd_rotation(new_dims, d, seed + rep_index), nodes of at
+ * least max_leaf points split at the mean of a rotated dimension drawn with
+ * probability proportional to its variance (the draw from a counter RNG
+ * keyed by the node), points below the mean first, then every bucket.  The
+ * node's own points give the statistics (the reference reads the first
+ * `size` entries of the whole permutation instead). */
+knng_status knng_run_rep_kd(knng_context* ctx, uint32_t max_leaf, uint32_t new_dims, uint64_t seed,
+                            uint32_t rep_index, knng_stats* stats);
+
+/* The rotation of the KD splitter, made on the host as rotateRandom makes it
+ * (src/SolutionRandomKD.hpp:258-264): new_dims vectors of d normal draws on a
+ * std::mt19937 seeded with `seed` (the reference's generator starts at
+ * 12345), each divided by its norm, then the reference's Gram-Schmidt
+ * (src/LinearAlgebra.hpp:211-222).  out: new_dims x d floats.  No device. */
+knng_status knng_kd_rotation(uint32_t new_dims, uint32_t d, uint64_t seed, float* out);
+
 /* Bucket-pass autotuner (no counterpart in the reference; the reference has a
  * single CPU loop, src/KnnSets.hpp:131-160).  Times the FP32 bucket-pass
  * variants on one repetition of the context's own points and current sets

@@ -93,6 +93,9 @@ def _olib():
         lib.ko_counter_position.argtypes = [c_uint64, c_uint32, c_uint32, c_uint32, c_uint32, c_uint32]
         lib.ko_counter_position.restype = c_uint32
         lib.ko_knnset_replay.argtypes = [c_uint32, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+        lib.ko_kd_vectors.argtypes = [c_uint32, c_uint32, c_uint64, c_void_p]
+        lib.ko_kd_rotate.argtypes = [c_void_p, c_void_p, c_uint32, c_void_p]
+        lib.ko_kd_rep.argtypes = [c_void_p, c_uint32, c_uint32, c_uint64, c_uint32]
         _oracle_lib = lib
     return _oracle_lib
 
@@ -107,6 +110,13 @@ def dot(a: np.ndarray, b: np.ndarray) -> float:
     a = np.ascontiguousarray(a, np.float32)
     b = np.ascontiguousarray(b, np.float32)
     return float(_olib().ko_dot(_ptr(a), _ptr(b), a.shape[0]))
+
+
+def kd_vectors(new_dims: int, d: int, seed: int) -> np.ndarray:
+    """The KD solution's rotation vectors (new_dims x d) from a mt19937 seeded with seed."""
+    out = np.zeros((new_dims, d), np.float32)
+    _olib().ko_kd_vectors(new_dims, d, seed, _ptr(out))
+    return out
 
 
 def sample_count(n: int) -> int:
@@ -162,6 +172,17 @@ class Oracle:
 
     def refine(self) -> int:
         return int(self._lib.ko_refine(self._h))
+
+    def kd_rep(self, max_leaf: int, new_dims: int = 30, seed: int = 12345, rep_index: int = 0) -> None:
+        """One repetition with the random-rotation KD splitter."""
+        self._lib.ko_kd_rep(self._h, max_leaf, new_dims, seed, rep_index)
+
+    def kd_rotate(self, vectors: np.ndarray) -> np.ndarray:
+        """rot[p, c] = dot(vectors[c], x_p) with the reference's dot."""
+        v = np.ascontiguousarray(vectors, np.float32)
+        out = np.zeros((self.n, v.shape[0]), np.float32)
+        self._lib.ko_kd_rotate(self._h, _ptr(v), v.shape[0], _ptr(out))
+        return out
 
     def lloyd(self, ids: np.ndarray, c1: np.ndarray, c2: np.ndarray, iters: int):
         """Lloyd steps over the point ids in the given order from centres c1, c2;
@@ -260,6 +281,7 @@ class ReferenceShim:
         lib.ref_distance.restype = c_float
         lib.ref_dot.argtypes = [c_void_p, c_void_p]
         lib.ref_dot.restype = c_float
+        lib.ref_kd_rotate.argtypes = [c_void_p, c_uint32, c_void_p]
         lib.ref_knnset_replay.argtypes = [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
         self._lib = lib
         pts = np.ascontiguousarray(points, np.float32)
@@ -286,6 +308,12 @@ class ReferenceShim:
 
     def topup(self) -> int:
         return int(self._lib.ref_topup(self._h))
+
+    def kd_rotate(self, new_dims: int = 30) -> np.ndarray:
+        """SolutionRandomKD::rotateRandom on a fresh thread (generator at its seed)."""
+        out = np.zeros((self.n, new_dims), np.float32)
+        self._lib.ref_kd_rotate(self._h, new_dims, _ptr(out))
+        return out
 
     def indices(self) -> np.ndarray:
         out = np.zeros(self.n, np.uint32)

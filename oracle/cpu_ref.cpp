@@ -396,6 +396,123 @@ void split_node(Oracle& o, uint32_t start, uint32_t end, uint32_t iters, uint32_
 
 }  // namespace
 
+// ------------------------------------------------------------ KD splitter
+//
+// Restatement of the random-rotation KD solution's repetition
+// (SolutionRandomKD::rotateRandom / split, src/SolutionRandomKD.hpp:258-375)
+// with the conventions of the library's KD splitter: the node's own points
+// give the statistics (the reference reads indices[0 .. size)), the dimension
+// draw comes from the counter RNG, a node with every point on one side is
+// redrawn up to 64 times and then halved at its index midpoint, and buckets
+// go through leaf_all_pairs (the 2-means form's set).
+
+// rotateRandom's vectors (src/SolutionRandomKD.hpp:258-264 with
+// randUniformUnitVec, normalizeInPlace and gramSchmidt,
+// src/LinearAlgebra.hpp:86-117, :211-222): per vector d normal draws on a
+// mt19937 seeded with `seed` (a new normal_distribution each), divided by the
+// square root of the float sum of float squares; then each vector minus its
+// float projections on the earlier ones, without rescaling (the reference's
+// normalize returns its argument).
+std::vector<float> kd_vectors(uint32_t nd, uint32_t d, uint64_t seed) {
+    std::mt19937 gen(static_cast<std::mt19937::result_type>(seed));
+    std::vector<std::vector<float>> v(nd, std::vector<float>(d));
+    for (uint32_t h = 0; h < nd; ++h) {
+        std::normal_distribution<> g(0, 1);
+        for (uint32_t i = 0; i < d; ++i) v[h][i] = static_cast<float>(g(gen));
+        float ss = 0.0f;
+        for (uint32_t i = 0; i < d; ++i) {
+            const float sq = v[h][i] * v[h][i];
+            ss += sq;
+        }
+        const double nrm = std::sqrt(static_cast<double>(ss));
+        for (uint32_t i = 0; i < d; ++i) v[h][i] = static_cast<float>(v[h][i] / nrm);
+    }
+    std::vector<float> out(static_cast<size_t>(nd) * d);
+    for (uint32_t i = 0; i < nd; ++i) {
+        std::vector<float> ui = v[i];
+        for (uint32_t j = 0; j < i; ++j) {
+            const float* uj = &out[static_cast<size_t>(j) * d];
+            const float s = canonical_dot(uj, v[i].data(), d);
+            for (uint32_t t = 0; t < d; ++t) {
+                const float prod = s * uj[t];
+                ui[t] = ui[t] - prod;
+            }
+        }
+        std::copy(ui.begin(), ui.end(), out.begin() + static_cast<size_t>(i) * d);
+    }
+    return out;
+}
+
+float kd_uniform(uint64_t seed, uint32_t rep, uint32_t start, uint32_t end, uint32_t attempt) {
+    uint64_t h = mix64(seed + 0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(rep) + 1));
+    h = mix64(h ^ ((static_cast<uint64_t>(start) << 32) | end));
+    h = mix64(h ^ ((static_cast<uint64_t>(attempt) << 32) | 0x4b44u));
+    return static_cast<float>(h >> 40) * 5.9604644775390625e-08f;
+}
+
+// pickIndexFull's choice (src/SolutionRandomKD.hpp:200-224).
+uint32_t kd_pick(const std::vector<double>& var, float u) {
+    std::vector<std::pair<double, uint32_t>> pairs;
+    float total = 0;
+    for (uint32_t j = 0; j < var.size(); ++j) {
+        pairs.emplace_back(var[j], j);
+        total += var[j];
+    }
+    std::sort(pairs.begin(), pairs.end(), std::greater{});
+    const float sample = u * total;
+    float so_far = 0;
+    for (auto& [v, j] : pairs) {
+        so_far += v;
+        if (so_far >= sample) return j;
+    }
+    return pairs.back().second;
+}
+
+struct KdState {
+    uint32_t nd = 0, max_leaf = 0;
+    uint64_t seed = 0;
+    std::vector<float> rot;  // n x nd
+};
+
+void kd_split(Oracle& o, const KdState& k, uint32_t start, uint32_t end, uint32_t attempt) {
+    const uint32_t size = end - start;
+    if (size < k.max_leaf) {
+        o.leaves.emplace_back(start, end);
+        leaf_all_pairs(o, start, end);
+        return;
+    }
+    std::vector<double> mean(k.nd), var(k.nd);
+    for (uint32_t c = 0; c < k.nd; ++c) {
+        double sum = 0;
+        for (uint32_t i = start; i < end; ++i) sum += k.rot[static_cast<size_t>(o.indices[i]) * k.nd + c];
+        mean[c] = sum / size;
+        double s2 = 0;
+        for (uint32_t i = start; i < end; ++i) {
+            const double diff = k.rot[static_cast<size_t>(o.indices[i]) * k.nd + c] - mean[c];
+            s2 += diff * diff;
+        }
+        var[c] = s2 / (size - 1);
+    }
+    const uint32_t dim = kd_pick(var, kd_uniform(k.seed, o.rep, start, end, attempt));
+    std::vector<uint32_t> first, second;
+    for (uint32_t i = start; i < end; ++i) {
+        const uint32_t id = o.indices[i];
+        (k.rot[static_cast<size_t>(id) * k.nd + dim] < mean[dim] ? first : second).push_back(id);
+    }
+    uint32_t mid = start + static_cast<uint32_t>(first.size());
+    std::copy(first.begin(), first.end(), o.indices.begin() + start);
+    std::copy(second.begin(), second.end(), o.indices.begin() + mid);
+    if (mid == start || mid == end) {
+        if (attempt + 1 < 64) {
+            kd_split(o, k, start, end, attempt + 1);
+            return;
+        }
+        mid = start + size / 2;
+    }
+    kd_split(o, k, start, mid, 0);
+    kd_split(o, k, mid, end, 0);
+}
+
 extern "C" {
 
 void* ko_create(const float* pts, uint32_t n, uint32_t d, uint32_t ld, uint32_t k, uint32_t rng_mode, uint64_t seed) {
@@ -623,4 +740,34 @@ void ko_knnset_replay(uint32_t k, const uint32_t* cand, const float* dist, uint3
     *out_bound = s.bound[0];
 }
 
+
+void ko_kd_vectors(uint32_t nd, uint32_t d, uint64_t seed, float* out) {
+    const std::vector<float> v = kd_vectors(nd, d, seed);
+    std::copy(v.begin(), v.end(), out);
+}
+
+// rot[p * nd + c] = dot(vectors[c], x_p) (the reference's dot).
+void ko_kd_rotate(void* h, const float* vectors, uint32_t nd, float* out) {
+    auto* o = static_cast<Oracle*>(h);
+    for (uint32_t p = 0; p < o->n; ++p)
+        for (uint32_t c = 0; c < nd; ++c)
+            out[static_cast<size_t>(p) * nd + c] = canonical_dot(vectors + static_cast<size_t>(c) * o->d, o->row(p), o->d);
+}
+
+// One repetition with the KD splitter (rotation from kd_vectors(nd, d, seed + rep)).
+void ko_kd_rep(void* h, uint32_t max_leaf, uint32_t nd, uint64_t seed, uint32_t rep_index) {
+    auto* o = static_cast<Oracle*>(h);
+    o->rep = rep_index;
+    o->trace.clear();
+    o->leaves.clear();
+    std::iota(o->indices.begin(), o->indices.end(), 0u);
+    KdState k;
+    k.nd = nd;
+    k.max_leaf = max_leaf;
+    k.seed = seed;
+    const std::vector<float> v = kd_vectors(nd, o->d, seed + rep_index);
+    k.rot.resize(static_cast<size_t>(o->n) * nd);
+    ko_kd_rotate(h, v.data(), nd, k.rot.data());
+    if (o->n > 0) kd_split(*o, k, 0, o->n, 0);
+}
 }  // extern "C"

@@ -18,8 +18,11 @@
 #include <fstream>
 #include <iostream>
 
+#include <thread>
+
 #include "ann.hpp"  // defines the processTime global the hot path updates
 #include "SolutionKmeans.hpp"
+#include "SolutionRandomKD.hpp"
 
 namespace {
 
@@ -149,6 +152,16 @@ void ref_knnset_replay(const uint32_t* cand_ids, const float* cand_dists, uint32
     *size = s.size;
     *lower_bound_idx = s.lowerBoundIdx;
     *bound = b;
+}
+
+// SolutionRandomKD::rotateRandom (src/SolutionRandomKD.hpp:258-275) on the
+// context's points, run on a fresh thread so that its thread_local generator
+// (src/Constants.hpp:22) starts from its seed: the rotated values, n rows of
+// new_dims floats, of the KD solution's first iteration.
+void ref_kd_rotate(void* ctx, uint32_t new_dims, float* out) {
+    auto* c = static_cast<RefCtx*>(ctx);
+    std::thread t([&] { SolutionRandomKD::rotateRandom(new_dims, c->n, c->points, out); });
+    t.join();
 }
 
 }  // extern "C"

@@ -33,7 +33,7 @@ PRECISION_BF16_RERANK = 1
 EXPORTED = [
     "knng_default_params", "knng_status_string", "knng_create", "knng_destroy", "knng_last_error", "knng_build",
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
-    "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_tune_buckets", "knng_get_leaves", "knng_refine",
+    "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_run_rep_kd", "knng_kd_rotation", "knng_tune_buckets", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
     "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_debug_set_wait_limit", "knng_refine_pointwise_noalloc",
     "knng_build_batch",
@@ -111,6 +111,8 @@ def load_library(path: str = LIB_PATH):
         "knng_lloyd": (c_int, [P, c_uint32, P, P, P, P, P, P, c_uint32, P, P, P]),
         "knng_process_leaves": (c_int, [P, c_uint32, P, P]),
         "knng_run_rep": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, c_uint32, POINTER(Stats)]),
+        "knng_run_rep_kd": (c_int, [P, c_uint32, c_uint32, c_uint64, c_uint32, POINTER(Stats)]),
+        "knng_kd_rotation": (c_int, [c_uint32, c_uint32, c_uint64, P]),
         "knng_tune_buckets": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, POINTER(ctypes.c_double),
                                       POINTER(c_uint32)]),
         "knng_get_leaves": (c_int, [P, c_uint32, P, P, P]),
@@ -351,6 +353,13 @@ class KnngContext:
                                            ctypes.byref(st)))
         return st
 
+    def run_rep_kd(self, max_leaf: int, new_dims: int = 30, seed: int = 12345, rep_index: int = 0,
+                   stats: Stats | None = None) -> Stats:
+        """knng_run_rep_kd: one repetition with the random-rotation KD splitter."""
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_run_rep_kd(self._h, max_leaf, new_dims, seed, rep_index, ctypes.byref(st)))
+        return st
+
     def tune_buckets(self, max_leaf: int, lloyd_iters: int, small_threshold: int = 3000,
                      seed: int = 12345) -> tuple[list[float], int]:
         """knng_tune_buckets: bucket-pass ms of the four variants (every pair /
@@ -532,3 +541,12 @@ class KnngServer:
 def job_reservation(n: int, d: int, k: int) -> int:
     """HBM bytes a served job of n points, d dims, k neighbours reserves."""
     return int(load_library().knng_job_reservation(n, d, k))
+
+
+def kd_rotation(new_dims: int, d: int, seed: int) -> np.ndarray:
+    """knng_kd_rotation: the KD splitter's rotation vectors (new_dims x d), host only."""
+    out = np.zeros((new_dims, d), np.float32)
+    status = load_library().knng_kd_rotation(new_dims, d, seed, out.ctypes.data_as(c_void_p))
+    if status != 0:
+        raise KnngError(status, "knng_kd_rotation refused its arguments")
+    return out

@@ -903,6 +903,50 @@ knng_status knng_run_rep(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_it
     });
 }
 
+knng_status knng_kd_rotation(uint32_t new_dims, uint32_t d, uint64_t seed, float* out) {
+    if (!out || new_dims < 1 || new_dims > 32 || !knng::dim_supported(d)) return KNNG_ERR_INVALID_ARGUMENT;
+    try {
+        const std::vector<float> r = knng::kd_rotation(new_dims, d, seed);
+        std::copy(r.begin(), r.end(), out);
+    } catch (...) {
+        return KNNG_ERR_OUT_OF_MEMORY;
+    }
+    return KNNG_OK;
+}
+
+knng_status knng_run_rep_kd(knng_context* ctx, uint32_t max_leaf, uint32_t new_dims, uint64_t seed,
+                            uint32_t rep_index, knng_stats* stats) {
+    return knng::guarded(ctx, [&](Context& c) {
+        if (max_leaf < 2 || max_leaf > 4097) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be in [2, 4097]");
+        knng::require_sets(c);
+        knng::KdRepResult res;
+        knng::run_rep_kd(c, max_leaf, new_dims, seed, rep_index, res);
+        std::vector<std::pair<uint32_t, uint32_t>> lv(res.leaf_start.size());
+        for (size_t i = 0; i < lv.size(); ++i) lv[i] = {res.leaf_start[i], res.leaf_end[i]};
+        std::sort(lv.begin(), lv.end());
+        c.last_leaf_start.resize(lv.size());
+        c.last_leaf_end.resize(lv.size());
+        for (size_t i = 0; i < lv.size(); ++i) {
+            c.last_leaf_start[i] = lv[i].first;
+            c.last_leaf_end[i] = lv[i].second;
+        }
+        knng::RepStats st;
+        st.levels = res.levels;
+        st.nodes = res.nodes;
+        st.restarts = res.restarts;
+        st.fallbacks = res.fallbacks;
+        st.ms_split = res.ms_split;
+        st.ms_leaf = res.ms_leaf;
+        knng::add_rep_stats(stats, st);
+        if (stats) {
+            stats->reps_done += 1;
+            stats->buckets += lv.size();
+            stats->leaf_launches += lv.empty() ? 0 : 1;
+            stats->ms_leaf_kernel += res.ms_leaf;
+        }
+    });
+}
+
 knng_status knng_tune_buckets(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_iters, uint32_t small_threshold,
                               uint64_t seed, double* out_ms, uint32_t* out_choice) {
     return knng::guarded(ctx, [&](Context& c) {

@@ -218,6 +218,16 @@ void launch_partition(Context& c, uint32_t count, const uint32_t* h_starts, cons
 // Device-side repetition (split.cu): the tree built by device-side levels,
 // as one CUDA graph (graph = true) or launched level by level, then the
 // bucket pass over the device's leaf list.
+// Random-rotation KD splitter (kd.cu): the rotation vectors of a repetition
+// (new_dims x d floats), and one repetition -- indices = iota, the KD tree,
+// the bucket pass over its leaves.
+std::vector<float> kd_rotation(uint32_t new_dims, uint32_t d, uint64_t seed);
+struct KdRepResult {
+    std::vector<uint32_t> leaf_start, leaf_end;
+    double ms_split = 0, ms_leaf = 0;
+    uint64_t levels = 0, nodes = 0, restarts = 0, fallbacks = 0;
+};
+void run_rep_kd(Context& c, uint32_t max_leaf, uint32_t new_dims, uint64_t seed, uint32_t rep, KdRepResult& out);
 struct DevRepResult {
     std::vector<uint32_t> leaf_start, leaf_end;  // in no particular order
     double ms_split = 0, ms_leaf = 0;

@@ -1,0 +1,338 @@
+// Random-rotation KD splitter: SolutionRandomKD (src/SolutionRandomKD.hpp:45-430),
+// the reference's alternative solution (disabled at src/main.cpp:58), as a
+// second splitter behind the same side test, stable partition and bucket pass
+// as the 2-means tree.
+//
+// One repetition (rotateRandom :258-275, split :284-375):
+//   * new_dims rotation vectors, made on the host as rotateRandom makes them:
+//     each of d normal draws (std::normal_distribution<double>(0, 1), a new
+//     distribution per vector, on a std::mt19937) rounded to float and divided
+//     by its norm (normalizeInPlace, src/LinearAlgebra.hpp:86-91: the norm is
+//     the square root of a float sum of float squares), then the reference's
+//     Gram-Schmidt (:211-222), whose normalize returns its input (:93-101), so
+//     that only the first vector has unit length; projections use the
+//     reference's dot (:179-200);
+//   * rotated values rot[p][c] = dot(u_c, x_p) on the device (k_kd_rotate),
+//     in the reference's dot order;
+//   * per node of at least max_leaf points: the mean and the (size - 1)
+//     variance of every rotated dimension in double, one point at a time in
+//     index order (pickIndexFull :196-224, getMean :92-114, getVariance
+//     :116-143); the dimension drawn with probability proportional to its
+//     variance (pairs sorted in descending order, a float running total, a
+//     uniform draw in [0, total) -- here from the counter RNG, keyed by the
+//     node, instead of the reference's generator); split value = that
+//     dimension's mean; the points with rot < mean first (:316-358).  The
+//     partition is the 2-means side test with coefficients -u and offset -F,
+//     F the largest float below the mean: dot(-u, x) >= -F is rot < mean bit
+//     for bit (negating every operand negates the dot exactly);
+//   * nodes below max_leaf points are buckets for the usual bucket pass.
+//
+// Deliberate differences.  The reference's getMean / getVariance read the
+// rows indices[0 .. size) -- the first `size` entries of the whole
+// permutation -- instead of the node's range, so its splits depend on the
+// final order of every node to its left (and on thread timing under TBB);
+// here the statistics are the node's own.  When every point falls on one
+// side the reference recurses on the same range; here the node is redrawn
+// (next attempt) up to 64 times, then split at its index midpoint.  Its
+// KnnSetScannable (src/KnnSets.hpp:225-282) overwrites the first maximum slot
+// in slot order; the bucket pass here uses the 2-means form's set (the same
+// offers in the same order and the same accepted candidates; ties at the
+// maximum resolved in getMaxIdx's order).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <random>
+#include <vector>
+
+#include "common.cuh"
+#include "context.hpp"
+#include "dispatch.hpp"
+
+namespace knng {
+
+namespace {
+
+constexpr uint32_t kMaxKdDims = 32;  // one lane per rotated dimension
+
+// The reference's dot (src/LinearAlgebra.hpp:179-200) for d values: eight FMA
+// chains over the dimensions below the last multiple of 8 (rhs * lhs + sum),
+// the lanes added left to right to 0, then each remaining product added.
+float host_ref_dot(const float* lhs, const float* rhs, uint32_t d) {
+    const uint32_t m = d / 8 * 8;
+    float lane[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t i = 0; i < m; i += 8)
+        for (int l = 0; l < 8; ++l) lane[l] = std::fma(rhs[i + l], lhs[i + l], lane[l]);
+    float ans = 0.0f;
+    for (int l = 0; l < 8; ++l) ans += lane[l];
+    for (uint32_t i = m; i < d; ++i) {
+        const float prod = lhs[i] * rhs[i];
+        ans += prod;
+    }
+    return ans;
+}
+
+// normalizeInPlace: v / sqrt(float sum of float squares), divided in double.
+void host_normalize(std::vector<float>& v) {
+    float sum_squares = 0.0f;
+    for (float x : v) {
+        const float sq = x * x;
+        sum_squares += sq;
+    }
+    const double norm = std::sqrt(static_cast<double>(sum_squares));
+    for (float& x : v) x = static_cast<float>(static_cast<double>(x) / norm);
+}
+
+}  // namespace
+
+std::vector<float> kd_rotation(uint32_t new_dims, uint32_t d, uint64_t seed) {
+    std::mt19937 rng(static_cast<std::mt19937::result_type>(seed));
+    std::vector<std::vector<float>> v(new_dims, std::vector<float>(d));
+    for (uint32_t h = 0; h < new_dims; ++h) {
+        std::normal_distribution<> normal(0, 1);
+        for (uint32_t i = 0; i < d; ++i) v[h][i] = static_cast<float>(normal(rng));
+        host_normalize(v[h]);
+    }
+    // gramSchmidt: u_i = v_i - sum_j dot(u_j, v_i) u_j, each subtraction of
+    // the float product rounded; no rescaling after the first vector.
+    std::vector<std::vector<float>> u(new_dims);
+    for (uint32_t i = 0; i < new_dims; ++i) {
+        u[i] = v[i];
+        for (uint32_t j = 0; j < i; ++j) {
+            const float s = host_ref_dot(u[j].data(), v[i].data(), d);
+            for (uint32_t k = 0; k < d; ++k) {
+                const float prod = s * u[j][k];
+                u[i][k] = u[i][k] - prod;
+            }
+        }
+    }
+    std::vector<float> out(static_cast<size_t>(new_dims) * d);
+    for (uint32_t i = 0; i < new_dims; ++i) std::copy(u[i].begin(), u[i].end(), out.begin() + static_cast<size_t>(i) * d);
+    return out;
+}
+
+namespace {
+
+// rot[p * nd + c] = dot(u_c, x_p) in the reference's order: one warp per
+// point, lane c < nd one dimension; the vectors sit in shared memory with row
+// stride D + 1 (conflict-free across lanes), the point's row is read as a
+// broadcast.
+template <int D>
+__global__ void __launch_bounds__(256) k_kd_rotate(const float* __restrict__ pts, int ld, uint32_t n,
+                                                   const float* __restrict__ rotation, uint32_t nd,
+                                                   float* __restrict__ rot) {
+    __shared__ float u_s[kMaxKdDims * (D + 1)];
+    __shared__ float x_s[8][D];
+    for (uint32_t f = threadIdx.x; f < nd * D; f += blockDim.x) u_s[(f / D) * (D + 1) + f % D] = rotation[f];
+    __syncthreads();
+    const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
+    constexpr int M = D / 8 * 8;
+    const float* u = u_s + lane * (D + 1);
+    for (uint32_t p = blockIdx.x * 8 + warp; p < n; p += gridDim.x * 8) {
+        for (int k = lane; k < D; k += kWarp) x_s[warp][k] = pts[static_cast<size_t>(p) * ld + k];
+        __syncwarp();
+        if (static_cast<uint32_t>(lane) < nd) {
+            const float* x = x_s[warp];
+            float chain[8];
+#pragma unroll
+            for (int l = 0; l < 8; ++l) chain[l] = 0.0f;
+#pragma unroll
+            for (int i = 0; i < M; i += 8)
+#pragma unroll
+                for (int l = 0; l < 8; ++l) chain[l] = __fmaf_rn(x[i + l], u[i + l], chain[l]);
+            float ans = 0.0f;
+#pragma unroll
+            for (int l = 0; l < 8; ++l) ans = __fadd_rn(ans, chain[l]);
+#pragma unroll
+            for (int i = M; i < D; ++i) ans = __fadd_rn(ans, __fmul_rn(u[i], x[i]));
+            rot[static_cast<size_t>(p) * nd + lane] = ans;
+        }
+        __syncwarp();
+    }
+}
+
+// Per node i (one warp): for every rotated dimension c < nd (lane c) the mean
+// and the (size - 1) variance of rot over the node's points, in double, one
+// point at a time in index order.
+__global__ void __launch_bounds__(kWarp) k_kd_stats(const uint32_t* __restrict__ starts,
+                                                    const uint32_t* __restrict__ ends,
+                                                    const uint32_t* __restrict__ idx,
+                                                    const float* __restrict__ rot, uint32_t nd,
+                                                    double* __restrict__ mean, double* __restrict__ var) {
+    const uint32_t node = blockIdx.x;
+    const uint32_t c = threadIdx.x;
+    const uint32_t lo = starts[node], hi = ends[node];
+    if (c >= nd) return;
+    double sum = 0.0;
+#pragma unroll 8
+    for (uint32_t i = lo; i < hi; ++i) sum = __dadd_rn(sum, static_cast<double>(rot[static_cast<size_t>(idx[i]) * nd + c]));
+    const double m = __ddiv_rn(sum, static_cast<double>(hi - lo));
+    double s2 = 0.0;
+#pragma unroll 8
+    for (uint32_t i = lo; i < hi; ++i) {
+        const double diff = __dsub_rn(static_cast<double>(rot[static_cast<size_t>(idx[i]) * nd + c]), m);
+        s2 = __dadd_rn(s2, __dmul_rn(diff, diff));
+    }
+    mean[static_cast<size_t>(node) * nd + c] = m;
+    var[static_cast<size_t>(node) * nd + c] = __ddiv_rn(s2, static_cast<double>(hi - lo - 1));
+}
+
+}  // namespace
+
+namespace {
+
+constexpr uint32_t kMaxKdAttempts = 64;
+
+// The uniform draw of a node's dimension pick: a float in [0, 1) from the
+// counter RNG keyed by (seed, repetition, node range, attempt).
+float kd_uniform(uint64_t seed, uint32_t rep, uint32_t start, uint32_t end, uint32_t attempt) {
+    uint64_t h = mix64(seed + 0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(rep) + 1));
+    h = mix64(h ^ ((static_cast<uint64_t>(start) << 32) | end));
+    h = mix64(h ^ ((static_cast<uint64_t>(attempt) << 32) | 0x4b44u));
+    return static_cast<float>(h >> 40) * 5.9604644775390625e-08f;  // 2^-24
+}
+
+// pickIndexFull's choice (src/SolutionRandomKD.hpp:200-224) from the node's
+// variances: pairs (variance, dimension) in descending order, a float running
+// total, the first dimension whose running sum reaches u * total.
+uint32_t kd_pick(const double* var, uint32_t nd, float u) {
+    std::vector<std::pair<double, uint32_t>> order;
+    float total = 0.0f;
+    for (uint32_t j = 0; j < nd; ++j) {
+        order.emplace_back(var[j], j);
+        total = static_cast<float>(static_cast<double>(total) + var[j]);
+    }
+    std::sort(order.begin(), order.end(), std::greater<>());
+    const float sample = u * total;
+    float so_far = 0.0f;
+    for (const auto& [v, j] : order) {
+        so_far = static_cast<float>(static_cast<double>(so_far) + v);
+        if (so_far >= sample) return j;
+    }
+    return order.back().second;  // the reference leaves this case undefined
+}
+
+// Largest float strictly below m.
+float float_below(double m) {
+    float f = static_cast<float>(m);
+    while (static_cast<double>(f) >= m) f = std::nextafter(f, -INFINITY);
+    return f;
+}
+
+}  // namespace
+
+void run_rep_kd(Context& c, uint32_t max_leaf, uint32_t new_dims, uint64_t seed, uint32_t rep, KdRepResult& out) {
+    if (new_dims < 1 || new_dims > kMaxKdDims) fail(KNNG_ERR_INVALID_ARGUMENT, "new_dims must be in [1, 32]");
+    if (max_leaf < 2) fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be >= 2");
+    const uint32_t n = c.n, d = c.d, nd = new_dims;
+    cudaEvent_t ev[3];
+    for (auto& e : ev) KNNG_CUDA(cudaEventCreate(&e));
+    KNNG_CUDA(cudaEventRecord(ev[0], c.stream));
+    // Rotation (repetition r uses the generator seeded with seed + r) and the
+    // rotated values.
+    const std::vector<float> rotation = kd_rotation(nd, d, seed + rep);
+    float* d_rotation = upload(c, "kd_rotation", rotation.data(), rotation.size());
+    auto* rot = static_cast<float*>(scratch(c, "kd_rot", static_cast<size_t>(n) * nd * sizeof(float)));
+    KNNG_DISPATCH_D(d, {
+        const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 7) / 8, c.sms * 16));
+        k_kd_rotate<D><<<blocks, 256, 0, c.stream>>>(c.points, c.ld, n, d_rotation, nd, rot);
+    });
+    ++c.launches;
+    KNNG_CUDA(cudaGetLastError());
+    launch_iota(c);
+    // Level by level: nodes of at least max_leaf points split, the others are
+    // buckets.
+    struct KdNode {
+        uint32_t start, end, attempt;
+    };
+    std::vector<KdNode> level;
+    std::vector<uint32_t> leaf_start, leaf_end;
+    auto place = [&](uint32_t s, uint32_t e, std::vector<KdNode>& next) {
+        if (e - s < max_leaf) {
+            leaf_start.push_back(s);
+            leaf_end.push_back(e);
+        } else {
+            next.push_back({s, e, 0});
+        }
+    };
+    for (size_t s = 0; s + 1 < c.set_offsets.size(); ++s) {
+        std::vector<KdNode> roots;
+        place(c.set_offsets[s], c.set_offsets[s + 1], roots);
+        level.insert(level.end(), roots.begin(), roots.end());
+    }
+    const uint32_t ld = c.ld;
+    while (!level.empty()) {
+        const uint32_t m = static_cast<uint32_t>(level.size());
+        out.levels += 1;
+        out.nodes += m;
+        std::vector<uint32_t> hs(m), he(m);
+        for (uint32_t i = 0; i < m; ++i) {
+            hs[i] = level[i].start;
+            he[i] = level[i].end;
+        }
+        uint32_t* d_s = upload(c, "kd_starts", hs.data(), m);
+        uint32_t* d_e = upload(c, "kd_ends", he.data(), m);
+        auto* d_mean = static_cast<double*>(scratch(c, "kd_mean", static_cast<size_t>(m) * nd * sizeof(double)));
+        auto* d_var = static_cast<double*>(scratch(c, "kd_var", static_cast<size_t>(m) * nd * sizeof(double)));
+        k_kd_stats<<<m, kWarp, 0, c.stream>>>(d_s, d_e, c.indices, rot, nd, d_mean, d_var);
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
+        std::vector<double> mean(static_cast<size_t>(m) * nd), var(static_cast<size_t>(m) * nd);
+        download(c, mean.data(), d_mean, mean.size());
+        download(c, var.data(), d_var, var.size());
+        // Hyperplanes: coefficients -u_dim, offset -F.
+        std::vector<float> coefs(static_cast<size_t>(m) * ld, 0.0f), offs(m);
+        for (uint32_t i = 0; i < m; ++i) {
+            const float u = kd_uniform(seed, rep, hs[i], he[i], level[i].attempt);
+            const uint32_t dim = kd_pick(&var[static_cast<size_t>(i) * nd], nd, u);
+            for (uint32_t k = 0; k < d; ++k) coefs[static_cast<size_t>(i) * ld + k] = -rotation[static_cast<size_t>(dim) * d + k];
+            offs[i] = -float_below(mean[static_cast<size_t>(i) * nd + dim]);
+        }
+        float* d_c = upload(c, "kd_coefs", coefs.data(), coefs.size());
+        float* d_o = upload(c, "kd_offsets", offs.data(), m);
+        auto* d_t = static_cast<uint32_t*>(scratch(c, "kd_true", m * sizeof(uint32_t)));
+        launch_partition(c, m, hs.data(), he.data(), d_s, d_c, d_o, d_t);
+        std::vector<uint32_t> t(m);
+        download(c, t.data(), d_t, m);
+        std::vector<KdNode> next;
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t s = hs[i], e = he[i];
+            uint32_t mid = s + t[i];
+            if (mid == s || mid == e) {  // every point on one side
+                if (level[i].attempt + 1 < kMaxKdAttempts) {
+                    next.push_back({s, e, level[i].attempt + 1});
+                    out.restarts += 1;
+                    continue;
+                }
+                mid = s + (e - s) / 2;  // the partition left the order unchanged
+                out.fallbacks += 1;
+            }
+            place(s, mid, next);
+            place(mid, e, next);
+        }
+        level.swap(next);
+    }
+    KNNG_CUDA(cudaEventRecord(ev[1], c.stream));
+    // The bucket pass over every leaf.
+    const uint32_t nl = static_cast<uint32_t>(leaf_start.size());
+    uint32_t max_bucket = 0;
+    for (uint32_t i = 0; i < nl; ++i) max_bucket = std::max(max_bucket, leaf_end[i] - leaf_start[i]);
+    if (nl > 0) {
+        uint32_t* d_ls = upload(c, "kd_leaf_start", leaf_start.data(), nl);
+        uint32_t* d_le = upload(c, "kd_leaf_end", leaf_end.data(), nl);
+        launch_leaves(c, nl, d_ls, d_le, max_bucket, nullptr);
+    }
+    KNNG_CUDA(cudaEventRecord(ev[2], c.stream));
+    KNNG_CUDA(cudaEventSynchronize(ev[2]));
+    float ms = 0.f;
+    KNNG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    out.ms_split = ms;
+    KNNG_CUDA(cudaEventElapsedTime(&ms, ev[1], ev[2]));
+    out.ms_leaf = ms;
+    for (auto& e : ev) cudaEventDestroy(e);
+    out.leaf_start = std::move(leaf_start);
+    out.leaf_end = std::move(leaf_end);
+}
+
+}  // namespace knng

@@ -71,7 +71,7 @@ def main() -> int:
         raw = f.read()
     with lzma.open(os.path.join(HERE, FIXTURE), "wb", preset=9) as f:
         f.write(raw)
-    golden = {"cases": {}, "arith": {}, "knnset": {}}
+    golden = {"cases": {}, "arith": {}, "knnset": {}, "kd_rotation": {}}
     for name, gen, reps, topup in CASES:
         pts = case_points(gen)
         ref = bindings.ReferenceShim(pts)
@@ -121,6 +121,19 @@ def main() -> int:
             "size": r["size"], "maxslot": r["maxslot"], "bound_bits": int(np.float32(r["bound"]).view(np.uint32)),
         }
     ref.close()
+    # SolutionRandomKD::rotateRandom (src/SolutionRandomKD.hpp:258-275) with
+    # the solution's 30 new dimensions (:390), its generator at the seed: the
+    # rotated values of the reference fixture and of a seeded mixture.
+    for name, gen in (("dummy_data", {"file": FIXTURE}),
+                      ("mix6k", dict(n=6000, d=100, clusters=16, sigma=0.15, seed=7))):
+        pts = case_points(gen)
+        ref = bindings.ReferenceShim(pts)
+        rot = ref.kd_rotate(30)
+        golden["kd_rotation"][name] = {
+            "generator": gen, "new_dims": 30, "seed": 12345, "digest": digest(rot),
+            "rows_bits": {str(r): rot[r].view(np.uint32).tolist() for r in (0, len(rot) - 1)},
+        }
+        ref.close()
     with open(OUT, "w") as f:
         json.dump(golden, f, indent=0, sort_keys=True)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")

@@ -171,3 +171,21 @@ def test_schedule_and_tuning_entry_points_refuse_null(knng_lib):
     assert knng_lib.knng_tune_buckets(None, 1025, 2, 3000, 1, ms, ctypes.byref(choice)) == 1
     assert knng_lib.knng_debug_set_wait_limit(None, 0) == 1
     assert knng_lib.knng_build_adaptive(None, None, 10, 100, 400, None, 0.9, 10, None, None, None) == 1
+
+
+def test_kd_rotation_entry_point_matches_oracle(knng_lib, oracle_lib):
+    """knng_kd_rotation (host only) makes the KD solution's rotation vectors
+    bit for bit as the oracle's restatement does, for several seeds and sizes;
+    out-of-range sizes are refused."""
+    import numpy as np
+
+    for nd, d, seed in [(30, 100, 12345), (8, 100, 7), (32, 100, 2**40 + 3), (1, 100, 0), (16, 128, 99)]:
+        mine = api.kd_rotation(nd, d, seed)
+        want = oracle_lib.kd_vectors(nd, d, seed)
+        assert np.array_equal(mine.view(np.uint32), want.view(np.uint32)), (nd, d, seed)
+    out = np.zeros(33 * 100, np.float32)
+    ptr = out.ctypes.data_as(ctypes.c_void_p)
+    assert knng_lib.knng_kd_rotation(33, 100, 1, ptr) == 1
+    assert knng_lib.knng_kd_rotation(0, 100, 1, ptr) == 1
+    assert knng_lib.knng_kd_rotation(4, 100, 1, None) == 1
+    assert knng_lib.knng_run_rep_kd(None, 400, 30, 1, 0, None) == 1

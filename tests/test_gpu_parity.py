@@ -611,3 +611,32 @@ def test_refine_long_survivor_lists_equal_pointwise(knng_lib, monkeypatch):
         b.refine()
         pointwise = b.sets()
     assert_sets_equal(joined, pointwise, "join vs pointwise, long lists")
+
+
+def test_kd_rep_matches_oracle(oracle_lib, ctx):
+    """knng_run_rep_kd (rotation on the host, rotated values, node statistics,
+    side test, stable partition and buckets on the device) equals the oracle's
+    KD restatement: permutation, buckets and sets after every repetition, then
+    the top-up and the final lists.  The second input has 1,500 copies of one
+    point, whose nodes have every point on one side until the midpoint split."""
+    mix = workloads.gaussian_mixture(n=12_000, d=100, clusters=24, sigma=0.15, seed=17)
+    dup = np.concatenate([np.repeat(mix[:1], 1500, axis=0), mix[:1500]])
+    for pts, reps in ((mix, [(400, 0), (257, 1), (400, 2)]), (dup, [(200, 0), (129, 5)])):
+        o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=12345)
+        ctx.load_points(pts)
+        ctx.reset_sets(100)
+        for leaf, r in reps:
+            o.kd_rep(leaf, 30, 12345, r)
+            ctx.run_rep_kd(leaf, 30, 12345, r)
+            np.testing.assert_array_equal(ctx.indices(), o.indices())
+            s, e = ctx.leaves()
+            t = o.trace()
+            order = np.argsort(t["leaf_start"])
+            np.testing.assert_array_equal(s, t["leaf_start"][order])
+            np.testing.assert_array_equal(e, t["leaf_end"][order])
+            assert_sets_equal(ctx.sets(), o.sets(), f"kd rep {r}")
+        assert ctx.refine() == o.refine()
+        ids, dist = ctx.finalize(want_dists=True)
+        oids, odist = o.finalize()
+        np.testing.assert_array_equal(ids, oids)
+        np.testing.assert_array_equal(dist.view(np.uint32), odist.view(np.uint32))

@@ -154,6 +154,54 @@ def test_oracle_equals_reference_on_fresh_input(oracle_lib):
         assert sets_digest(ref.sets()) == sets_digest(o.sets())
 
 
+def test_kd_rotation_matches_reference_golden(oracle_lib, golden):
+    """The restated rotateRandom (vectors from the seeded mt19937, the
+    reference's normalisation and Gram-Schmidt, its dot) reproduces the
+    reference's rotated values bit for bit."""
+    for name, g in golden["kd_rotation"].items():
+        pts = case_points(g["generator"])
+        o = oracle_lib.Oracle(pts, k=10)
+        rot = o.kd_rotate(oracle_lib.kd_vectors(g["new_dims"], pts.shape[1], g["seed"]))
+        assert digest(rot) == g["digest"], name
+        for row, bits in g["rows_bits"].items():
+            assert rot[int(row)].view(np.uint32).tolist() == bits
+
+
+def test_kd_oracle_buckets_and_degenerate_input(oracle_lib):
+    """The KD restatement tiles the points with buckets below max_leaf and
+    fills every set from its bucket; identical points (zero variance, every
+    split one-sided) end in midpoint splits."""
+    pts = workloads.gaussian_mixture(n=3000, d=100, clusters=8, sigma=0.2, seed=4)
+    o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=5)
+    o.kd_rep(300, 30, 5, 0)
+    idx = o.indices()
+    assert np.array_equal(np.sort(idx), np.arange(3000))
+    t = o.trace()
+    order = np.argsort(t["leaf_start"])
+    s, e = t["leaf_start"][order], t["leaf_end"][order]
+    assert s[0] == 0 and e[-1] == 3000 and np.array_equal(s[1:], e[:-1])
+    assert (e - s).max() < 300
+    size = o.sets()["size"]
+    for a, b in zip(s, e):
+        assert (size[idx[a:b]] == min(100, b - a - 1)).all()
+    same = np.ones((700, 100), np.float32)
+    o2 = oracle_lib.Oracle(same, k=10, rng_mode=1, seed=1)
+    o2.kd_rep(200, 30, 1, 0)
+    t2 = o2.trace()
+    assert sorted(zip(t2["leaf_start"].tolist(), t2["leaf_end"].tolist())) == [(0, 175), (175, 350), (350, 525),
+                                                                               (525, 700)]
+
+
+@pytest.mark.skipif(not os.path.isdir(__import__("oracle.bindings").bindings.REFERENCE_SRC),
+                    reason="needs the reference tree")
+def test_kd_rotation_equals_reference_on_fresh_input(oracle_lib):
+    pts = workloads.gaussian_mixture(n=2000, d=100, clusters=5, sigma=0.3, seed=31)
+    ref = oracle_lib.ReferenceShim(pts)
+    want = ref.kd_rotate(30)
+    got = oracle_lib.Oracle(pts, k=10).kd_rotate(oracle_lib.kd_vectors(30, 100, 12345))
+    assert np.array_equal(want.view(np.uint32), got.view(np.uint32))
+
+
 def test_workload_generators():
     a = workloads.gaussian_mixture(1000, 100, 8, 0.15, seed=0)
     b = workloads.gaussian_mixture(1000, 100, 8, 0.15, seed=0)
