@@ -77,6 +77,8 @@ def parse_args(argv=None):
     ap.add_argument("--max-leaf", type=int, default=0, help="leaf test bound (0: 1025, buckets of at most 1024)")
     ap.add_argument("--precision", action="store_true",
                     help="measure only the precision form against the FP32 form (100k-point config)")
+    ap.add_argument("--kd", action="store_true",
+                    help="measure only the KD splitter beside the 2-means splitter")
     ap.add_argument("--batched-waves", type=int, default=5, help="waves of the batched form to run (of 5)")
     return ap.parse_args(argv)
 
@@ -505,6 +507,50 @@ def run_precision(device: int = 0, steps: int = 3, cpu_reference: bool = True) -
     return out
 
 
+# ------------------------------------------------------------ KD splitter
+
+def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MAX_LEAF) -> dict:
+    """The random-rotation KD splitter (30 rotated dimensions) beside the
+    2-means splitter on the bench's points: `reps` repetitions of each from
+    empty sets, buckets below max_leaf, then one neighbour-of-neighbour pass;
+    device time of the split stage and of the bucket pass (CUDA events on the
+    library's stream), recall on sampled points against FP64 brute force."""
+    import torch
+
+    from sigmod23ann_b200 import KnngContext, Stats, groundtruth, workloads
+
+    x = workloads.subspace_mixture_torch(n, seed=SEED, device=f"cuda:{device}")
+    q = np.random.default_rng(SEED).choice(n, min(2000, n), replace=False)
+    gt = groundtruth.exact_knn_torch(x, q, K)
+    host = x.cpu().numpy()
+    x = None
+    torch.cuda.empty_cache()
+    out = {"workload": f"{n:,} x {DIM} f32 subspace mixture (seed {SEED}), k={K}, buckets < {max_leaf}, "
+                       f"{reps} repetitions + 1 pass, recall on {len(q):,} points"}
+    with KnngContext(device) as ctx:
+        ctx.load_points(host)
+        for name in ("two_means", "kd"):
+            ctx.reset_sets(K)
+            split = leaf = 0.0
+            buckets = 0
+            for r in range(reps):
+                st = Stats()
+                if name == "kd":
+                    ctx.run_rep_kd(max_leaf, 30, SEED, r, st)
+                else:
+                    ctx.run_rep(max_leaf, LLOYD_ITERS, 3000, SEED, r, st)
+                split += st.ms_split
+                leaf += st.ms_leaf
+                buckets += st.buckets
+            st = Stats()
+            ctx.refine(st)
+            ids = ctx.finalize()
+            out[name] = {"split_ms_per_rep": sig(split / reps), "bucket_ms_per_rep": sig(leaf / reps),
+                         "buckets_per_rep": buckets // reps, "refine_ms": sig(st.ms_refine),
+                         "recall": sig(groundtruth.recall(ids.astype(np.int64), gt, q))}
+    return out
+
+
 # ------------------------------------------------------------ batched arm
 
 def batched_sets(seed: int = 2, count: int = 4096):
@@ -772,7 +818,8 @@ def run_ours(args):
     if extras and args.extras:
         for key, fn in (("precision", lambda: precision_summary(run_precision(local, 3, cpu_reference=False))),
                         ("batched", lambda: batched_summary(run_batched(1, local))),
-                        ("serving", lambda: serving_summary(run_serving_pair(args.serving_requests, local)))):
+                        ("serving", lambda: serving_summary(run_serving_pair(args.serving_requests, local))),
+                        ("kd_splitter", lambda: run_kd_compare(n, local, args.reps, max_leaf))):
             try:
                 line[key] = fn()
             except Exception as e:  # an extra figure must not hide the build number
@@ -813,6 +860,12 @@ def main(argv=None):
         print(json.dumps({"metric": "points/sec, batched k-NN graph builds (4,096 sets)", "value": res["points_per_s"],
                           "unit": "points/s", "higher_is_better": True, "n_gpus": 1, "dtype": "f32",
                           "batched": res}))
+        return 0
+    if args.kd:
+        res = run_kd_compare(args.n, 0, args.reps, args.max_leaf or MAX_LEAF)
+        print(json.dumps({"metric": "KD splitter beside the 2-means splitter: ms per repetition, recall",
+                          "value": res["kd"]["split_ms_per_rep"] + res["kd"]["bucket_ms_per_rep"], "unit": "ms",
+                          "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "kd_splitter": res}))
         return 0
     if args.serving:
         res = run_serving_pair(max(1, args.serving_requests))

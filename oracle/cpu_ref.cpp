@@ -481,15 +481,29 @@ void kd_split(Oracle& o, const KdState& k, uint32_t start, uint32_t end, uint32_
         leaf_all_pairs(o, start, end);
         return;
     }
+    // getMean / getVariance (src/SolutionRandomKD.hpp:93-143) sum per TBB
+    // block and combine in thread order; here the order is fixed: chunks of
+    // 1,024 positions from the node's start, each summed in index order from
+    // 0, then the chunk sums in chunk order.
+    constexpr uint32_t kChunk = 1024;
     std::vector<double> mean(k.nd), var(k.nd);
     for (uint32_t c = 0; c < k.nd; ++c) {
+        auto value = [&](uint32_t i) { return static_cast<double>(k.rot[static_cast<size_t>(o.indices[i]) * k.nd + c]); };
         double sum = 0;
-        for (uint32_t i = start; i < end; ++i) sum += k.rot[static_cast<size_t>(o.indices[i]) * k.nd + c];
+        for (uint32_t b = start; b < end; b += kChunk) {
+            double part = 0;
+            for (uint32_t i = b; i < std::min(end, b + kChunk); ++i) part += value(i);
+            sum += part;
+        }
         mean[c] = sum / size;
         double s2 = 0;
-        for (uint32_t i = start; i < end; ++i) {
-            const double diff = k.rot[static_cast<size_t>(o.indices[i]) * k.nd + c] - mean[c];
-            s2 += diff * diff;
+        for (uint32_t b = start; b < end; b += kChunk) {
+            double part = 0;
+            for (uint32_t i = b; i < std::min(end, b + kChunk); ++i) {
+                const double diff = value(i) - mean[c];
+                part += diff * diff;
+            }
+            s2 += part;
         }
         var[c] = s2 / (size - 1);
     }

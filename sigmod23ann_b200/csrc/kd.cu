@@ -15,9 +15,11 @@
 //   * rotated values rot[p][c] = dot(u_c, x_p) on the device (k_kd_rotate),
 //     in the reference's dot order;
 //   * per node of at least max_leaf points: the mean and the (size - 1)
-//     variance of every rotated dimension in double, one point at a time in
-//     index order (pickIndexFull :196-224, getMean :92-114, getVariance
-//     :116-143); the dimension drawn with probability proportional to its
+//     variance of every rotated dimension in double (pickIndexFull :196-224,
+//     getMean :92-114, getVariance :116-143), summed in a fixed order -- per
+//     chunk of 1,024 positions in index order, then the chunk sums in chunk
+//     order (the reference sums per TBB block and combines in thread order,
+//     so its order is not fixed); the dimension drawn with probability proportional to its
 //     variance (pairs sorted in descending order, a float running total, a
 //     uniform draw in [0, total) -- here from the counter RNG, keyed by the
 //     node, instead of the reference's generator); split value = that
@@ -152,30 +154,58 @@ __global__ void __launch_bounds__(256) k_kd_rotate(const float* __restrict__ pts
     }
 }
 
-// Per node i (one warp): for every rotated dimension c < nd (lane c) the mean
-// and the (size - 1) variance of rot over the node's points, in double, one
-// point at a time in index order.
-__global__ void __launch_bounds__(kWarp) k_kd_stats(const uint32_t* __restrict__ starts,
-                                                    const uint32_t* __restrict__ ends,
-                                                    const uint32_t* __restrict__ idx,
-                                                    const float* __restrict__ rot, uint32_t nd,
-                                                    double* __restrict__ mean, double* __restrict__ var) {
-    const uint32_t node = blockIdx.x;
-    const uint32_t c = threadIdx.x;
-    const uint32_t lo = starts[node], hi = ends[node];
-    if (c >= nd) return;
-    double sum = 0.0;
+// Node statistics in a fixed order that does not depend on the launch: a
+// node's positions in chunks of kKdChunk; each chunk's values added one at a
+// time in index order to a double starting at 0 (k_kd_chunk_sums, one warp per
+// chunk, lane c one rotated dimension), then the chunk sums one at a time in
+// chunk order (k_kd_node_stats, one warp per node).  With `mean` null the
+// values are rot; otherwise (rot - mean)^2 in double.
+constexpr uint32_t kKdChunk = 1024;
+constexpr int kKdWarps = 8;
+
+struct KdChunk {
+    uint32_t node, begin, end;
+};
+
+__global__ void __launch_bounds__(kKdWarps * kWarp) k_kd_chunk_sums(const KdChunk* __restrict__ chunks, uint32_t count,
+                                                                    const uint32_t* __restrict__ idx,
+                                                                    const float* __restrict__ rot, uint32_t nd,
+                                                                    const double* __restrict__ mean,
+                                                                    double* __restrict__ partial) {
+    const uint32_t item = blockIdx.x * kKdWarps + threadIdx.x / kWarp;
+    const uint32_t c = threadIdx.x % kWarp;
+    if (item >= count || c >= nd) return;
+    const KdChunk ch = chunks[item];
+    double s = 0.0;
+    if (mean == nullptr) {
 #pragma unroll 8
-    for (uint32_t i = lo; i < hi; ++i) sum = __dadd_rn(sum, static_cast<double>(rot[static_cast<size_t>(idx[i]) * nd + c]));
-    const double m = __ddiv_rn(sum, static_cast<double>(hi - lo));
-    double s2 = 0.0;
+        for (uint32_t i = ch.begin; i < ch.end; ++i)
+            s = __dadd_rn(s, static_cast<double>(rot[static_cast<size_t>(idx[i]) * nd + c]));
+    } else {
+        const double m = mean[static_cast<size_t>(ch.node) * nd + c];
 #pragma unroll 8
-    for (uint32_t i = lo; i < hi; ++i) {
-        const double diff = __dsub_rn(static_cast<double>(rot[static_cast<size_t>(idx[i]) * nd + c]), m);
-        s2 = __dadd_rn(s2, __dmul_rn(diff, diff));
+        for (uint32_t i = ch.begin; i < ch.end; ++i) {
+            const double diff = __dsub_rn(static_cast<double>(rot[static_cast<size_t>(idx[i]) * nd + c]), m);
+            s = __dadd_rn(s, __dmul_rn(diff, diff));
+        }
     }
-    mean[static_cast<size_t>(node) * nd + c] = m;
-    var[static_cast<size_t>(node) * nd + c] = __ddiv_rn(s2, static_cast<double>(hi - lo - 1));
+    partial[static_cast<size_t>(item) * nd + c] = s;
+}
+
+// out[node][c] = (sum of the node's chunk sums in chunk order) / divisor,
+// divisor = size (means) or size - 1 (variances).
+__global__ void __launch_bounds__(kKdWarps * kWarp) k_kd_node_stats(const uint32_t* __restrict__ first_chunk,
+                                                                    const uint32_t* __restrict__ sizes, uint32_t m,
+                                                                    const double* __restrict__ partial, uint32_t nd,
+                                                                    uint32_t minus, double* __restrict__ out) {
+    const uint32_t node = blockIdx.x * kKdWarps + threadIdx.x / kWarp;
+    const uint32_t c = threadIdx.x % kWarp;
+    if (node >= m || c >= nd) return;
+    double s = 0.0;
+#pragma unroll 8
+    for (uint32_t j = first_chunk[node]; j < first_chunk[node + 1]; ++j)
+        s = __dadd_rn(s, partial[static_cast<size_t>(j) * nd + c]);
+    out[static_cast<size_t>(node) * nd + c] = __ddiv_rn(s, static_cast<double>(sizes[node] - minus));
 }
 
 }  // namespace
@@ -272,11 +302,29 @@ void run_rep_kd(Context& c, uint32_t max_leaf, uint32_t new_dims, uint64_t seed,
             he[i] = level[i].end;
         }
         uint32_t* d_s = upload(c, "kd_starts", hs.data(), m);
-        uint32_t* d_e = upload(c, "kd_ends", he.data(), m);
+        // Chunks of every node of the level, in node order.
+        std::vector<KdChunk> chunks;
+        std::vector<uint32_t> first(m + 1), sizes(m);
+        for (uint32_t i = 0; i < m; ++i) {
+            first[i] = static_cast<uint32_t>(chunks.size());
+            sizes[i] = he[i] - hs[i];
+            for (uint32_t b = hs[i]; b < he[i]; b += std::min(kKdChunk, he[i] - b))
+                chunks.push_back({i, b, b + std::min(kKdChunk, he[i] - b)});
+        }
+        first[m] = static_cast<uint32_t>(chunks.size());
+        const uint32_t nc = first[m];
+        const KdChunk* d_chunks = upload(c, "kd_chunks", chunks.data(), nc);
+        const uint32_t* d_first = upload(c, "kd_first_chunk", first.data(), m + 1);
+        const uint32_t* d_sizes = upload(c, "kd_sizes", sizes.data(), m);
+        auto* d_partial = static_cast<double*>(scratch(c, "kd_partial", static_cast<size_t>(nc) * nd * sizeof(double)));
         auto* d_mean = static_cast<double*>(scratch(c, "kd_mean", static_cast<size_t>(m) * nd * sizeof(double)));
         auto* d_var = static_cast<double*>(scratch(c, "kd_var", static_cast<size_t>(m) * nd * sizeof(double)));
-        k_kd_stats<<<m, kWarp, 0, c.stream>>>(d_s, d_e, c.indices, rot, nd, d_mean, d_var);
-        ++c.launches;
+        const uint32_t cb = (nc + kKdWarps - 1) / kKdWarps, nb = (m + kKdWarps - 1) / kKdWarps;
+        k_kd_chunk_sums<<<cb, kKdWarps * kWarp, 0, c.stream>>>(d_chunks, nc, c.indices, rot, nd, nullptr, d_partial);
+        k_kd_node_stats<<<nb, kKdWarps * kWarp, 0, c.stream>>>(d_first, d_sizes, m, d_partial, nd, 0, d_mean);
+        k_kd_chunk_sums<<<cb, kKdWarps * kWarp, 0, c.stream>>>(d_chunks, nc, c.indices, rot, nd, d_mean, d_partial);
+        k_kd_node_stats<<<nb, kKdWarps * kWarp, 0, c.stream>>>(d_first, d_sizes, m, d_partial, nd, 1, d_var);
+        c.launches += 4;
         KNNG_CUDA(cudaGetLastError());
         std::vector<double> mean(static_cast<size_t>(m) * nd), var(static_cast<size_t>(m) * nd);
         download(c, mean.data(), d_mean, mean.size());
