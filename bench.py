@@ -529,6 +529,13 @@ def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MA
                        f"{reps} repetitions + 1 pass, recall on {len(q):,} points"}
     with KnngContext(device) as ctx:
         ctx.load_points(host)
+        # One untimed repetition and pass first: the context's first pass
+        # allocates its scratch and loads the kernels.
+        ctx.reset_sets(K)
+        ctx.run_rep(max_leaf, LLOYD_ITERS, 3000, SEED, 0)
+        st = Stats()
+        ctx.refine(st)
+        out["first_refine_ms"] = sig(st.ms_refine)
         for name in ("two_means", "kd"):
             ctx.reset_sets(K)
             split = leaf = 0.0
