@@ -509,6 +509,55 @@ def run_precision(device: int = 0, steps: int = 3, cpu_reference: bool = True) -
 
 # ------------------------------------------------------------ KD splitter
 
+def refine_breakdown(st) -> dict:
+    """One neighbour-of-neighbour pass's device time by stage (ms) and its
+    survivor records that went past the pool to the per-point pass."""
+    return {"ms": sig(st.ms_refine), "prep": sig(st.ms_refine_prep), "join": sig(st.ms_refine_join),
+            "replay": sig(st.ms_refine_apply), "per_point": sig(st.ms_refine_fallback),
+            "overflow": int(st.refine_overflow), "changed": int(st.refine_changed)}
+
+
+def reference_kd_child(n: int, max_leaf: int, target_s: float) -> dict:
+    """In a child process (the reference's KD split recurses without end on
+    some inputs): one iteration of the reference's KD loop (rotateRandom +
+    split, all host threads) on a prefix of the bench's points, the prefix
+    grown until the iteration takes about target_s / 2."""
+    from oracle import bindings
+
+    cores = int(os.environ.setdefault("KNNG_REF_THREADS", str(os.cpu_count() or 1)))
+    pool = reference_prefix(n, min(n, 2_000_000))
+    m = min(len(pool), 20_000)
+    while True:
+        ref = bindings.ReferenceShim(pool[:m], threaded=True)
+        t = time.perf_counter()
+        ref.kd_reps(30, max_leaf, 1)
+        dt = time.perf_counter() - t
+        ref.close()
+        if dt >= target_s / 2 or m >= len(pool):
+            break
+        m = min(len(pool), int(m * min(8.0, max(1.5, target_s / max(dt, 1e-3)))))
+    return {"points_per_s_per_rep": sig(m / dt), "seconds": sig(dt), "sample_points": m, "cores": cores,
+            "kind": "reference", "sample": f"SolutionRandomKD rotateRandom + split (30 dims, buckets < {max_leaf}), one "
+                                          f"iteration from empty sets, first {m:,} points"}
+
+
+def reference_kd_rate(n: int, max_leaf: int, target_s: float = 10.0) -> dict:
+    from oracle import bindings
+
+    if not bindings.reference_available():
+        return {"unavailable": "the reference was not compiled here"}
+    code = (f"import json, sys; sys.path.insert(0, {ROOT!r}); import bench; "
+            f"print(json.dumps(bench.reference_kd_child({n}, {max_leaf}, {target_s})))")
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=20 * target_s + 120,
+                           env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out"}
+    if r.returncode != 0:
+        return {"error": f"exit {r.returncode}: {r.stderr.strip()[-160:]}"}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MAX_LEAF) -> dict:
     """The random-rotation KD splitter (30 rotated dimensions) beside the
     2-means splitter on the bench's points: `reps` repetitions of each from
@@ -535,7 +584,7 @@ def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MA
         ctx.run_rep(max_leaf, LLOYD_ITERS, 3000, SEED, 0)
         st = Stats()
         ctx.refine(st)
-        out["first_refine_ms"] = sig(st.ms_refine)
+        out["first_pass"] = refine_breakdown(st)
         for name in ("two_means", "kd"):
             ctx.reset_sets(K)
             split = leaf = 0.0
@@ -553,7 +602,7 @@ def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MA
             ctx.refine(st)
             ids = ctx.finalize()
             out[name] = {"split_ms_per_rep": sig(split / reps), "bucket_ms_per_rep": sig(leaf / reps),
-                         "buckets_per_rep": buckets // reps, "refine_ms": sig(st.ms_refine),
+                         "buckets_per_rep": buckets // reps, "pass": refine_breakdown(st),
                          "recall": sig(groundtruth.recall(ids.astype(np.int64), gt, q))}
     return out
 
@@ -870,6 +919,11 @@ def main(argv=None):
         return 0
     if args.kd:
         res = run_kd_compare(args.n, 0, args.reps, args.max_leaf or MAX_LEAF)
+        if not args.no_cpu_baseline:
+            cpu = reference_kd_rate(args.n, args.max_leaf or MAX_LEAF, args.cpu_seconds)
+            kd = res["kd"]
+            cpu["gpu_points_per_s_per_rep"] = sig(args.n / ((kd["split_ms_per_rep"] + kd["bucket_ms_per_rep"]) / 1e3))
+            res["cpu_baseline"] = cpu
         print(json.dumps({"metric": "KD splitter beside the 2-means splitter: ms per repetition, recall",
                           "value": res["kd"]["split_ms_per_rep"] + res["kd"]["bucket_ms_per_rep"], "unit": "ms",
                           "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "kd_splitter": res}))

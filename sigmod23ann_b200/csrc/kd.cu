@@ -35,7 +35,9 @@
 // final order of every node to its left (and on thread timing under TBB);
 // here the statistics are the node's own.  When every point falls on one
 // side the reference recurses on the same range; here the node is redrawn
-// (next attempt) up to 64 times, then split at its index midpoint.  Its
+// (next attempt) up to 64 times, then split at its index midpoint.  The
+// reference gathers each side per TBB block and concatenates the blocks in
+// combine order (:331-351); here each side keeps index order (stable).  Its
 // KnnSetScannable (src/KnnSets.hpp:225-282) overwrites the first maximum slot
 // in slot order; the bucket pass here uses the 2-means form's set (the same
 // offers in the same order and the same accepted candidates; ties at the
