@@ -514,48 +514,30 @@ def refine_breakdown(st) -> dict:
     survivor records that went past the pool to the per-point pass."""
     return {"ms": sig(st.ms_refine), "prep": sig(st.ms_refine_prep), "join": sig(st.ms_refine_join),
             "replay": sig(st.ms_refine_apply), "per_point": sig(st.ms_refine_fallback),
-            "overflow": int(st.refine_overflow), "changed": int(st.refine_changed)}
+            "overflow": int(st.refine_overflow), "changed": int(st.refine_changed),
+            "pairs": int(st.refine_pairs), "filter_kept": int(st.refine_filter_pass),
+            "exact": int(st.refine_exact), "survivors": int(st.refine_emits)}
 
 
-def reference_kd_child(n: int, max_leaf: int, target_s: float) -> dict:
-    """In a child process (the reference's KD split recurses without end on
-    some inputs): one iteration of the reference's KD loop (rotateRandom +
-    split, all host threads) on a prefix of the bench's points, the prefix
-    grown until the iteration takes about target_s / 2."""
+def oracle_kd_rate(n: int, max_leaf: int, target_s: float) -> dict:
+    """The oracle's KD repetition (the C++ restatement, one host thread) on a
+    prefix of the bench's points, grown until one repetition takes about
+    target_s / 2: rotation, node statistics, partition, buckets."""
     from oracle import bindings
 
-    cores = int(os.environ.setdefault("KNNG_REF_THREADS", str(os.cpu_count() or 1)))
     pool = reference_prefix(n, min(n, 2_000_000))
     m = min(len(pool), 20_000)
     while True:
-        ref = bindings.ReferenceShim(pool[:m], threaded=True)
+        o = bindings.Oracle(pool[:m], k=K, rng_mode=1, seed=SEED)
         t = time.perf_counter()
-        ref.kd_reps(30, max_leaf, 1)
+        o.kd_rep(max_leaf, 30, SEED, 0)
         dt = time.perf_counter() - t
-        ref.close()
+        o.close()
         if dt >= target_s / 2 or m >= len(pool):
             break
         m = min(len(pool), int(m * min(8.0, max(1.5, target_s / max(dt, 1e-3)))))
-    return {"points_per_s_per_rep": sig(m / dt), "seconds": sig(dt), "sample_points": m, "cores": cores,
-            "kind": "reference", "sample": f"SolutionRandomKD rotateRandom + split (30 dims, buckets < {max_leaf}), one "
-                                          f"iteration from empty sets, first {m:,} points"}
-
-
-def reference_kd_rate(n: int, max_leaf: int, target_s: float = 10.0) -> dict:
-    from oracle import bindings
-
-    if not bindings.reference_available():
-        return {"unavailable": "the reference was not compiled here"}
-    code = (f"import json, sys; sys.path.insert(0, {ROOT!r}); import bench; "
-            f"print(json.dumps(bench.reference_kd_child({n}, {max_leaf}, {target_s})))")
-    try:
-        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=20 * target_s + 120,
-                           env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
-    except subprocess.TimeoutExpired:
-        return {"error": "timed out"}
-    if r.returncode != 0:
-        return {"error": f"exit {r.returncode}: {r.stderr.strip()[-160:]}"}
-    return json.loads(r.stdout.strip().splitlines()[-1])
+    return {"points_per_s_per_rep": sig(m / dt), "seconds": sig(dt), "sample_points": m, "cores": 1, "kind": "port",
+            "sample": f"oracle KD repetition (30 dims, buckets < {max_leaf}) from empty sets, first {m:,} points"}
 
 
 def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MAX_LEAF) -> dict:
@@ -864,6 +846,12 @@ def run_ours(args):
             "clocks": {k: clock[k] for k in ("sm_mhz", "sm_max_mhz", "reasons") if k in clock},
             "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "bucket_tuning": tuning,
             "stages_ms_last_step": stages,
+            # The joins' pair funnel in the last step (both passes): pairs
+            # evaluated, pairs the tensor-core bound kept, of those already in
+            # the point's list, exact distances, survivor records.
+            "join_pairs_last_step": {k: int(last[v]) for k, v in (
+                ("pairs", "refine_pairs"), ("filter_kept", "refine_filter_pass"),
+                ("members", "refine_member_skip"), ("exact", "refine_exact"), ("survivors", "refine_emits"))},
         }
         if adaptive is not None:
             line["adaptive"] = adaptive
@@ -920,7 +908,7 @@ def main(argv=None):
     if args.kd:
         res = run_kd_compare(args.n, 0, args.reps, args.max_leaf or MAX_LEAF)
         if not args.no_cpu_baseline:
-            cpu = reference_kd_rate(args.n, args.max_leaf or MAX_LEAF, args.cpu_seconds)
+            cpu = oracle_kd_rate(args.n, args.max_leaf or MAX_LEAF, args.cpu_seconds)
             kd = res["kd"]
             cpu["gpu_points_per_s_per_rep"] = sig(args.n / ((kd["split_ms_per_rep"] + kd["bucket_ms_per_rep"]) / 1e3))
             res["cpu_baseline"] = cpu

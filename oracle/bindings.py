@@ -282,7 +282,6 @@ class ReferenceShim:
         lib.ref_dot.argtypes = [c_void_p, c_void_p]
         lib.ref_dot.restype = c_float
         lib.ref_kd_rotate.argtypes = [c_void_p, c_uint32, c_void_p]
-        lib.ref_kd_reps.argtypes = [c_void_p, c_uint32, c_uint32, c_uint32]
         lib.ref_knnset_replay.argtypes = [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
         self._lib = lib
         pts = np.ascontiguousarray(points, np.float32)
@@ -309,10 +308,6 @@ class ReferenceShim:
 
     def topup(self) -> int:
         return int(self._lib.ref_topup(self._h))
-
-    def kd_reps(self, new_dims: int = 30, max_group: int = 400, reps: int = 1) -> None:
-        """`reps` iterations of the KD solution's loop (rotate, split) with its own sets."""
-        self._lib.ref_kd_reps(self._h, new_dims, max_group, reps)
 
     def kd_rotate(self, new_dims: int = 30) -> np.ndarray:
         """SolutionRandomKD::rotateRandom on a fresh thread (generator at its seed)."""

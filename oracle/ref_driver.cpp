@@ -7,7 +7,7 @@
 //   SolutionKmeans::splitKmeansBinaryProcess   src/SolutionKmeans.hpp:142-311
 //   SolutionKmeans::topUpSingle                src/SolutionKmeans.hpp:480-555
 //   KnnSetScannableSimd::finalize + padResult  src/KnnSets.hpp:113-126, :334-344
-//   SolutionRandomKD::rotateRandom / split      src/SolutionRandomKD.hpp:258-375
+//   SolutionRandomKD::rotateRandom              src/SolutionRandomKD.hpp:258-275
 // with fixed parameters instead of the reference's wall-clock loop
 // (src/SolutionKmeans.hpp:579-602).  Built by oracle/Makefile into
 // oracle/_ref/ (never committed): libref_serial.so pins the oracle,
@@ -18,7 +18,6 @@
 #include <cstring>
 #include <fstream>
 #include <iostream>
-#include <numeric>
 
 #include <thread>
 
@@ -164,25 +163,6 @@ void ref_kd_rotate(void* ctx, uint32_t new_dims, float* out) {
     auto* c = static_cast<RefCtx*>(ctx);
     std::thread t([&] { SolutionRandomKD::rotateRandom(new_dims, c->n, c->points, out); });
     t.join();
-}
-
-// `reps` iterations of the KD solution's loop (src/SolutionRandomKD.hpp:
-// 395-413: iota, rotateRandom, split with its own KnnSetScannable sets) on
-// the context's points, for timing the reference's CPU KD form.  The sets
-// start empty and are dropped afterwards.
-void ref_kd_reps(void* ctx, uint32_t new_dims, uint32_t max_group_size, uint32_t reps) {
-    auto* c = static_cast<RefCtx*>(ctx);
-    CoutSilencer quiet;
-    std::vector<KnnSetScannable> sets(c->n);
-    std::vector<uint32_t> indices(c->n);
-    auto* rotated = static_cast<float*>(std::aligned_alloc(64, (static_cast<size_t>(c->n) * new_dims * sizeof(float) + 63) / 64 * 64));
-    for (uint32_t r = 0; r < reps; ++r) {
-        std::iota(indices.begin(), indices.end(), 0u);
-        SolutionRandomKD::rotateRandom(new_dims, c->n, c->points, rotated);
-        SolutionRandomKD::split(new_dims, c->n, std::vector<uint32_t>(), {0, c->n}, max_group_size, c->points, rotated,
-                                indices, sets);
-    }
-    std::free(rotated);
 }
 
 }  // extern "C"
