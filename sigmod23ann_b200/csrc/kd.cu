@@ -19,14 +19,17 @@
 //     getMean :92-114, getVariance :116-143), summed in a fixed order -- per
 //     chunk of 1,024 positions in index order, then the chunk sums in chunk
 //     order (the reference sums per TBB block and combines in thread order,
-//     so its order is not fixed); the dimension drawn with probability proportional to its
-//     variance (pairs sorted in descending order, a float running total, a
-//     uniform draw in [0, total) -- here from the counter RNG, keyed by the
-//     node, instead of the reference's generator); split value = that
-//     dimension's mean; the points with rot < mean first (:316-358).  The
-//     partition is the 2-means side test with coefficients -u and offset -F,
-//     F the largest float below the mean: dot(-u, x) >= -F is rot < mean bit
-//     for bit (negating every operand negates the dot exactly);
+//     so its order is not fixed); the dimension drawn with probability
+//     proportional to its variance (pairs sorted in descending order, a float
+//     running total, a uniform draw in [0, total) -- here from the counter
+//     RNG, keyed by the node, instead of the reference's generator); split
+//     value = that dimension's mean; the points with rot < mean first
+//     (:316-358).  Statistics, pick and hyperplane stay on the device
+//     (k_kd_chunk_sums, k_kd_node_stats, k_kd_pick); the host reads back only
+//     each node's side count.  The partition is the 2-means side test with
+//     coefficients -u and offset -F, F the largest float below the mean:
+//     dot(-u, x) >= -F is rot < mean bit for bit (negating every operand
+//     negates the dot exactly);
 //   * nodes below max_leaf points are buckets for the usual bucket pass.
 //
 // Deliberate differences.  The reference's getMean / getVariance read the
@@ -218,38 +221,59 @@ constexpr uint32_t kMaxKdAttempts = 64;
 
 // The uniform draw of a node's dimension pick: a float in [0, 1) from the
 // counter RNG keyed by (seed, repetition, node range, attempt).
-float kd_uniform(uint64_t seed, uint32_t rep, uint32_t start, uint32_t end, uint32_t attempt) {
+__device__ __forceinline__ float kd_uniform(uint64_t seed, uint32_t rep, uint32_t start, uint32_t end,
+                                            uint32_t attempt) {
     uint64_t h = mix64(seed + 0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(rep) + 1));
     h = mix64(h ^ ((static_cast<uint64_t>(start) << 32) | end));
     h = mix64(h ^ ((static_cast<uint64_t>(attempt) << 32) | 0x4b44u));
-    return static_cast<float>(h >> 40) * 5.9604644775390625e-08f;  // 2^-24
+    return __fmul_rn(static_cast<float>(h >> 40), 5.9604644775390625e-08f);  // 2^-24
 }
 
-// pickIndexFull's choice (src/SolutionRandomKD.hpp:200-224) from the node's
-// variances: pairs (variance, dimension) in descending order, a float running
-// total, the first dimension whose running sum reaches u * total.
-uint32_t kd_pick(const double* var, uint32_t nd, float u) {
-    std::vector<std::pair<double, uint32_t>> order;
+// Per node of a level (one warp): pickIndexFull's choice
+// (src/SolutionRandomKD.hpp:200-224) from the node's variances -- the float
+// total of the variances in dimension order, the pairs (variance, dimension)
+// in descending order (lane c's rank: the pairs above it), a float running
+// sum in that order, the first dimension whose running sum reaches u * total
+// (the last one if none does) -- then the node's hyperplane: coefficients
+// -u_dim and offset -F, F the largest float below the dimension's mean.
+__global__ void __launch_bounds__(kKdWarps * kWarp) k_kd_pick(const uint32_t* __restrict__ starts,
+                                                              const uint32_t* __restrict__ ends,
+                                                              const uint32_t* __restrict__ attempts, uint32_t m,
+                                                              const double* __restrict__ mean,
+                                                              const double* __restrict__ var, uint32_t nd,
+                                                              const float* __restrict__ rotation, uint32_t d, int ld,
+                                                              uint64_t seed, uint32_t rep, float* __restrict__ coefs,
+                                                              float* __restrict__ offs) {
+    const uint32_t node = blockIdx.x * kKdWarps + threadIdx.x / kWarp;
+    const uint32_t lane = threadIdx.x % kWarp;
+    if (node >= m) return;  // warp-uniform
+    const double v = lane < nd ? var[static_cast<size_t>(node) * nd + lane] : 0.0;
     float total = 0.0f;
+    uint32_t rank = 0;
     for (uint32_t j = 0; j < nd; ++j) {
-        order.emplace_back(var[j], j);
-        total = static_cast<float>(static_cast<double>(total) + var[j]);
+        const double vj = __shfl_sync(kFull, v, static_cast<int>(j));
+        total = __double2float_rn(__dadd_rn(static_cast<double>(total), vj));
+        rank += (vj > v || (vj == v && j > lane)) ? 1u : 0u;
     }
-    std::sort(order.begin(), order.end(), std::greater<>());
-    const float sample = u * total;
+    const float sample = __fmul_rn(kd_uniform(seed, rep, starts[node], ends[node], attempts[node]), total);
     float so_far = 0.0f;
-    for (const auto& [v, j] : order) {
-        so_far = static_cast<float>(static_cast<double>(so_far) + v);
-        if (so_far >= sample) return j;
+    uint32_t dim = 0;
+    for (uint32_t i = 0; i < nd; ++i) {
+        const unsigned who = __ballot_sync(kFull, lane < nd && rank == i);
+        if (who == 0) break;  // only with NaN variances: keep the last dimension found
+        dim = static_cast<uint32_t>(__ffs(who) - 1);
+        so_far = __double2float_rn(__dadd_rn(static_cast<double>(so_far), __shfl_sync(kFull, v, static_cast<int>(dim))));
+        if (so_far >= sample) break;  // warp-uniform
     }
-    return order.back().second;  // the reference leaves this case undefined
-}
-
-// Largest float strictly below m.
-float float_below(double m) {
-    float f = static_cast<float>(m);
-    while (static_cast<double>(f) >= m) f = std::nextafter(f, -INFINITY);
-    return f;
+    const double mu = mean[static_cast<size_t>(node) * nd + dim];
+    for (uint32_t k = lane; k < static_cast<uint32_t>(ld); k += kWarp)
+        coefs[static_cast<size_t>(node) * ld + k] = k < d ? -rotation[static_cast<size_t>(dim) * d + k] : 0.0f;
+    if (lane == 0) {
+        float f = __double2float_rn(mu);
+        // The nearest float is at most one step above the mean.
+        for (int t = 0; t < 4 && static_cast<double>(f) >= mu; ++t) f = nextafterf(f, -INFINITY);
+        offs[node] = -f;
+    }
 }
 
 }  // namespace
@@ -328,19 +352,17 @@ void run_rep_kd(Context& c, uint32_t max_leaf, uint32_t new_dims, uint64_t seed,
         k_kd_node_stats<<<nb, kKdWarps * kWarp, 0, c.stream>>>(d_first, d_sizes, m, d_partial, nd, 1, d_var);
         c.launches += 4;
         KNNG_CUDA(cudaGetLastError());
-        std::vector<double> mean(static_cast<size_t>(m) * nd), var(static_cast<size_t>(m) * nd);
-        download(c, mean.data(), d_mean, mean.size());
-        download(c, var.data(), d_var, var.size());
-        // Hyperplanes: coefficients -u_dim, offset -F.
-        std::vector<float> coefs(static_cast<size_t>(m) * ld, 0.0f), offs(m);
-        for (uint32_t i = 0; i < m; ++i) {
-            const float u = kd_uniform(seed, rep, hs[i], he[i], level[i].attempt);
-            const uint32_t dim = kd_pick(&var[static_cast<size_t>(i) * nd], nd, u);
-            for (uint32_t k = 0; k < d; ++k) coefs[static_cast<size_t>(i) * ld + k] = -rotation[static_cast<size_t>(dim) * d + k];
-            offs[i] = -float_below(mean[static_cast<size_t>(i) * nd + dim]);
-        }
-        float* d_c = upload(c, "kd_coefs", coefs.data(), coefs.size());
-        float* d_o = upload(c, "kd_offsets", offs.data(), m);
+        // Dimension picks and hyperplanes on the device.
+        std::vector<uint32_t> att(m);
+        for (uint32_t i = 0; i < m; ++i) att[i] = level[i].attempt;
+        const uint32_t* d_e = upload(c, "kd_ends", he.data(), m);
+        const uint32_t* d_att = upload(c, "kd_attempts", att.data(), m);
+        auto* d_c = static_cast<float*>(scratch(c, "kd_coefs", static_cast<size_t>(m) * ld * sizeof(float)));
+        auto* d_o = static_cast<float*>(scratch(c, "kd_offsets", m * sizeof(float)));
+        k_kd_pick<<<nb, kKdWarps * kWarp, 0, c.stream>>>(d_s, d_e, d_att, m, d_mean, d_var, nd, d_rotation, d, ld, seed,
+                                                         rep, d_c, d_o);
+        ++c.launches;
+        KNNG_CUDA(cudaGetLastError());
         auto* d_t = static_cast<uint32_t*>(scratch(c, "kd_true", m * sizeof(uint32_t)));
         launch_partition(c, m, hs.data(), he.data(), d_s, d_c, d_o, d_t);
         std::vector<uint32_t> t(m);
