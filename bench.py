@@ -545,7 +545,8 @@ def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MA
     2-means splitter on the bench's points: `reps` repetitions of each from
     empty sets, buckets below max_leaf, then one neighbour-of-neighbour pass;
     device time of the split stage and of the bucket pass (CUDA events on the
-    library's stream), recall on sampled points against FP64 brute force."""
+    library's stream), recall on sampled points against FP64 brute force after
+    every repetition and after the pass."""
     import torch
 
     from sigmod23ann_b200 import KnngContext, Stats, groundtruth, workloads
@@ -571,6 +572,7 @@ def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MA
             ctx.reset_sets(K)
             split = leaf = 0.0
             buckets = 0
+            per_rep = []
             for r in range(reps):
                 st = Stats()
                 if name == "kd":
@@ -580,10 +582,12 @@ def run_kd_compare(n: int, device: int = 0, reps: int = REPS, max_leaf: int = MA
                 split += st.ms_split
                 leaf += st.ms_leaf
                 buckets += st.buckets
+                per_rep.append(sig(groundtruth.recall(ctx.finalize().astype(np.int64), gt, q)))
             st = Stats()
             ctx.refine(st)
             ids = ctx.finalize()
-            out[name] = {"split_ms_per_rep": sig(split / reps), "bucket_ms_per_rep": sig(leaf / reps),
+            out[name] = {"recall_after_each_rep": per_rep,
+                         "split_ms_per_rep": sig(split / reps), "bucket_ms_per_rep": sig(leaf / reps),
                          "buckets_per_rep": buckets // reps, "pass": refine_breakdown(st),
                          "recall": sig(groundtruth.recall(ids.astype(np.int64), gt, q))}
     return out
