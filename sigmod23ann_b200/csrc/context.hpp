@@ -115,10 +115,6 @@ struct Context {
     bool refine_skip_old = true;
     bool snap_prev_valid = false;
     int64_t refine_pool = -1;
-    // Survivor records per point (all pool regions together) the join's pool
-    // holds when the budget allows; doubled after a pass whose pool regions
-    // filled up.
-    uint32_t pool_per_point = 128;
     // Breakdown of the last refinement pass.
     struct RefineRecord {
         double ms_join = 0, ms_apply = 0, ms_fallback = 0, ms_prep = 0;

@@ -1422,14 +1422,10 @@ uint64_t run_refine(Context& c) {
         pool_cap = static_cast<uint32_t>(c.refine_pool);
     } else {
         const uint64_t after = avail > static_cast<uint64_t>(n) * slots * 8 ? avail - static_cast<uint64_t>(n) * slots * 8 : 0;
-        // Half of what the slots leave, and at most c.pool_per_point records
-        // per point in all (so that a context's first pass maps no more
-        // memory than passes need): with fewer slots (a smaller budget) more
-        // records go to the pool, and a region that fills sends its points to
-        // the slow per-point pass (and doubles c.pool_per_point).
-        const uint64_t by_need = static_cast<uint64_t>(c.pool_per_point) * n / kJoinBlocks + 1;
-        pool_cap = static_cast<uint32_t>(
-            std::min<uint64_t>({after / 2 / (kJoinBlocks * 16ull), by_need, 1ull << 30}));
+        // Half of what the slots leave: with fewer slots (a smaller budget)
+        // more records go to the pool, and a region that fills sends its
+        // points to the slow per-point pass.
+        pool_cap = static_cast<uint32_t>(std::min<uint64_t>(after / 2 / (kJoinBlocks * 16ull), 1u << 30));
     }
     auto* scount = static_cast<uint32_t*>(scratch(c, "surv_count", static_cast<size_t>(n) * sizeof(uint32_t)));
     auto* ocount = static_cast<uint32_t*>(scratch(c, "surv_excess", static_cast<size_t>(n) * sizeof(uint32_t)));
@@ -1548,7 +1544,6 @@ uint64_t run_refine(Context& c) {
     // one-warp-per-point pass over their list.
     uint64_t changed_lost = 0;
     float ms_lost = 0.f;
-    if (lost_points > 0 && c.refine_pool < 0 && c.pool_per_point < (1u << 14)) c.pool_per_point *= 2;
     if (lost_points > 0) {
         cudaEvent_t r1, r2;
         KNNG_CUDA(cudaEventCreate(&r1));
