@@ -34,3 +34,14 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] == 2
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
     assert d["config"]["workload"].startswith("20,000 x 100 f32")
+
+
+def test_kd_cpu_baseline_leg_times_the_oracle_port():
+    """The --kd line's CPU baseline: the oracle's KD repetition on a prefix of
+    the bench's points, one host thread."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    r = bench.oracle_kd_rate(3000, 257, 0.2)
+    assert r["kind"] == "port" and r["cores"] == 1
+    assert r["sample_points"] == 3000 and r["points_per_s_per_rep"] > 0
