@@ -307,7 +307,7 @@ __device__ __forceinline__ void warp_bitonic_sort(unsigned long long* keys, uint
     for (uint32_t k = 2; k <= n; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             for (uint32_t t = lane; t < n / 2; t += kWarp) {
-                const uint32_t i = 2 * j * (t / j) + (t % j);
+                const uint32_t i = 2 * t - (t & (j - 1));  // 2 j (t / j) + t % j, j a power of two
                 const uint32_t partner = i + j;
                 const bool up = (i & k) == 0;
                 const unsigned long long a = keys[i], b = keys[partner];

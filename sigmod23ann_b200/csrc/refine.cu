@@ -1126,7 +1126,7 @@ __global__ void __launch_bounds__(kBigCtaThreads)
         for (uint32_t k = 2; k <= P2; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
                 for (uint32_t t = tid; t < P2 / 2; t += kBigCtaThreads) {
-                    const uint32_t i = 2 * j * (t / j) + (t % j);
+                    const uint32_t i = 2 * t - (t & (j - 1));  // 2 j (t / j) + t % j, j a power of two
                     const uint32_t partner = i + j;
                     const bool up = (i & k) == 0;
                     const unsigned long long a = keys[i], b = keys[partner];
