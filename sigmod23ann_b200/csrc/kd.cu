@@ -121,39 +121,72 @@ std::vector<float> kd_rotation(uint32_t new_dims, uint32_t d, uint64_t seed) {
 
 namespace {
 
-// rot[p * nd + c] = dot(u_c, x_p) in the reference's order: one warp per
-// point, lane c < nd one dimension; the vectors sit in shared memory with row
-// stride D + 1 (conflict-free across lanes), the point's row is read as a
-// broadcast.
+// rot[p * nd + c] = dot(u_c, x_p) in the reference's order: one warp per pair
+// of points, lane c < nd one rotated dimension.  The vectors sit in shared
+// memory with row stride kKdStride<D> (a multiple of 4 that is 4 mod 32, so
+// the lanes' 16-byte loads of a quarter-warp hit distinct bank groups); the
+// two rows are read as 16-byte broadcasts.  Each step of eight dimensions
+// takes two vector loads and two row loads per point for sixteen FMAs; chain
+// l (dimensions l, l + 8, ...) and the order of the sums are the reference's.
+template <int D>
+constexpr int kKdStride = D + (36 - D % 32) % 32;
+
 template <int D>
 __global__ void __launch_bounds__(256) k_kd_rotate(const float* __restrict__ pts, int ld, uint32_t n,
                                                    const float* __restrict__ rotation, uint32_t nd,
                                                    float* __restrict__ rot) {
-    __shared__ float u_s[kMaxKdDims * (D + 1)];
-    __shared__ float x_s[8][D];
-    for (uint32_t f = threadIdx.x; f < nd * D; f += blockDim.x) u_s[(f / D) * (D + 1) + f % D] = rotation[f];
+    constexpr int S = kKdStride<D>;
+    static_assert(S % 4 == 0 && S % 32 == 4 && S >= D, "vector row stride");
+    __shared__ __align__(16) float u_s[kMaxKdDims * S];
+    __shared__ __align__(16) float x_s[8][2][D];
+    for (uint32_t f = threadIdx.x; f < nd * D; f += blockDim.x) u_s[(f / D) * S + f % D] = rotation[f];
     __syncthreads();
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
     constexpr int M = D / 8 * 8;
-    const float* u = u_s + lane * (D + 1);
-    for (uint32_t p = blockIdx.x * 8 + warp; p < n; p += gridDim.x * 8) {
-        for (int k = lane; k < D; k += kWarp) x_s[warp][k] = pts[static_cast<size_t>(p) * ld + k];
+    constexpr int Q = D / 4;
+    const float* u = u_s + lane * S;
+    for (uint32_t p0 = (blockIdx.x * 8 + warp) * 2; p0 < n; p0 += gridDim.x * 16) {
+        for (int f = lane; f < 2 * Q; f += kWarp) {
+            const uint32_t p = p0 + static_cast<uint32_t>(f / Q);
+            const float4 v = p < n ? *reinterpret_cast<const float4*>(pts + static_cast<size_t>(p) * ld + 4 * (f % Q))
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+            *reinterpret_cast<float4*>(&x_s[warp][f / Q][4 * (f % Q)]) = v;
+        }
         __syncwarp();
         if (static_cast<uint32_t>(lane) < nd) {
-            const float* x = x_s[warp];
-            float chain[8];
+            float chain[2][8];
 #pragma unroll
-            for (int l = 0; l < 8; ++l) chain[l] = 0.0f;
+            for (int q = 0; q < 2; ++q)
 #pragma unroll
-            for (int i = 0; i < M; i += 8)
+                for (int l = 0; l < 8; ++l) chain[q][l] = 0.0f;
+#pragma unroll 4
+            for (int i = 0; i < M; i += 8) {
+                const float4 ua = *reinterpret_cast<const float4*>(u + i);
+                const float4 ub = *reinterpret_cast<const float4*>(u + i + 4);
 #pragma unroll
-                for (int l = 0; l < 8; ++l) chain[l] = __fmaf_rn(x[i + l], u[i + l], chain[l]);
-            float ans = 0.0f;
+                for (int q = 0; q < 2; ++q) {
+                    const float4 xa = *reinterpret_cast<const float4*>(&x_s[warp][q][i]);
+                    const float4 xb = *reinterpret_cast<const float4*>(&x_s[warp][q][i + 4]);
+                    chain[q][0] = __fmaf_rn(xa.x, ua.x, chain[q][0]);
+                    chain[q][1] = __fmaf_rn(xa.y, ua.y, chain[q][1]);
+                    chain[q][2] = __fmaf_rn(xa.z, ua.z, chain[q][2]);
+                    chain[q][3] = __fmaf_rn(xa.w, ua.w, chain[q][3]);
+                    chain[q][4] = __fmaf_rn(xb.x, ub.x, chain[q][4]);
+                    chain[q][5] = __fmaf_rn(xb.y, ub.y, chain[q][5]);
+                    chain[q][6] = __fmaf_rn(xb.z, ub.z, chain[q][6]);
+                    chain[q][7] = __fmaf_rn(xb.w, ub.w, chain[q][7]);
+                }
+            }
 #pragma unroll
-            for (int l = 0; l < 8; ++l) ans = __fadd_rn(ans, chain[l]);
+            for (int q = 0; q < 2; ++q) {
+                const uint32_t p = p0 + static_cast<uint32_t>(q);
+                float ans = 0.0f;
 #pragma unroll
-            for (int i = M; i < D; ++i) ans = __fadd_rn(ans, __fmul_rn(u[i], x[i]));
-            rot[static_cast<size_t>(p) * nd + lane] = ans;
+                for (int l = 0; l < 8; ++l) ans = __fadd_rn(ans, chain[q][l]);
+#pragma unroll
+                for (int i = M; i < D; ++i) ans = __fadd_rn(ans, __fmul_rn(u[i], x_s[warp][q][i]));
+                if (p < n) rot[static_cast<size_t>(p) * nd + lane] = ans;
+            }
         }
         __syncwarp();
     }
@@ -291,7 +324,7 @@ void run_rep_kd(Context& c, uint32_t max_leaf, uint32_t new_dims, uint64_t seed,
     float* d_rotation = upload(c, "kd_rotation", rotation.data(), rotation.size());
     auto* rot = static_cast<float*>(scratch(c, "kd_rot", static_cast<size_t>(n) * nd * sizeof(float)));
     KNNG_DISPATCH_D(d, {
-        const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 7) / 8, c.sms * 16));
+        const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((n + 15) / 16, c.sms * 8));
         k_kd_rotate<D><<<blocks, 256, 0, c.stream>>>(c.points, c.ld, n, d_rotation, nd, rot);
     });
     ++c.launches;
