@@ -216,6 +216,20 @@ knng_status knng_run_rep(knng_context* ctx, uint32_t max_leaf, uint32_t lloyd_it
 knng_status knng_run_rep_kd(knng_context* ctx, uint32_t max_leaf, uint32_t new_dims, uint64_t seed,
                             uint32_t rep_index, knng_stats* stats);
 
+/* A whole build with the KD splitter, replacing
+ * SolutionRandomKD::constructResult (src/SolutionRandomKD.hpp:377-430: five
+ * iterations of rotateRandom + split with buckets below 400 points, then
+ * finalize + padResult): loads the points (as knng_build), empty sets of
+ * params->k, params->reps knng_run_rep_kd repetitions (rep_index 0, 1, ...;
+ * buckets below max_leaf, or max_leaf_odd on odd repetitions when nonzero),
+ * params->refine neighbour-of-neighbour passes (the reference's KD form has
+ * none), then the sorted, padded lists as knng_build writes them.
+ * params->precision must be KNNG_PRECISION_FP32; lloyd_iters and
+ * small_threshold are not used.  new_dims: 1..32 (the reference: 30). */
+knng_status knng_build_kd(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                          const knng_params* params, uint32_t new_dims, uint32_t* out_ids, float* out_dists,
+                          knng_stats* stats);
+
 /* The rotation of the KD splitter, made on the host as rotateRandom makes it
  * (src/SolutionRandomKD.hpp:258-264): new_dims vectors of d normal draws on a
  * std::mt19937 seeded with `seed` (the reference's generator starts at

@@ -59,6 +59,31 @@ void constructResult(float points[][Stride], uint32_t numPoints, std::vector<std
         result[i].assign(ids.begin() + static_cast<size_t>(i) * p.k, ids.begin() + static_cast<size_t>(i + 1) * p.k);
 }
 
+// The reference's alternative solution, SolutionRandomKD::constructResult
+// (src/SolutionRandomKD.hpp:377-430): five repetitions of the random-rotation
+// KD split (30 rotated dimensions, buckets below 400 points), no
+// neighbour-of-neighbour pass, then the sorted, padded lists.
+template <int Stride>
+void constructResultKD(float points[][Stride], uint32_t numPoints, std::vector<std::vector<uint32_t>>& result,
+                       const knng_params* params = nullptr, uint32_t new_dims = 30, uint32_t dims = 100,
+                       int device = 0) {
+    knng_params p;
+    knng_default_params(&p);
+    p.reps = 5;
+    p.max_leaf = 400;
+    p.max_leaf_odd = 0;
+    p.refine = 0;
+    if (params) p = *params;
+    Context ctx(device);
+    std::vector<uint32_t> ids(static_cast<size_t>(numPoints) * p.k);
+    Context::check(knng_build_kd(ctx.get(), &points[0][0], numPoints, dims, sizeof(float) * Stride, &p, new_dims,
+                                 ids.data(), nullptr, nullptr),
+                   ctx.get());
+    result.resize(numPoints);
+    for (uint32_t i = 0; i < numPoints; ++i)
+        result[i].assign(ids.begin() + static_cast<size_t>(i) * p.k, ids.begin() + static_cast<size_t>(i + 1) * p.k);
+}
+
 // The reference's schedule by wall clock (src/SolutionKmeans.hpp:579-604):
 // repetitions while less than build_ms has passed (the reference: 1,210 s, or
 // 20 s on its local runs), then refinement passes while less than

@@ -13,5 +13,6 @@ from .api import (  # noqa: F401
     construct_result,
     default_params,
     job_reservation,
+    kd_params,
     load_library,
 )

@@ -33,7 +33,7 @@ PRECISION_BF16_RERANK = 1
 EXPORTED = [
     "knng_default_params", "knng_status_string", "knng_create", "knng_destroy", "knng_last_error", "knng_build",
     "knng_build_device", "knng_load_points", "knng_reset_sets", "knng_begin_rep", "knng_split_nodes",
-    "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_run_rep_kd", "knng_kd_rotation", "knng_tune_buckets", "knng_get_leaves", "knng_refine",
+    "knng_farthest_pair", "knng_lloyd", "knng_process_leaves", "knng_run_rep", "knng_run_rep_kd", "knng_build_kd", "knng_kd_rotation", "knng_tune_buckets", "knng_get_leaves", "knng_refine",
     "knng_get_indices", "knng_set_indices", "knng_get_sets", "knng_set_sets", "knng_finalize",
     "knng_debug_tile_gram", "knng_debug_tile_gram_bf16", "knng_debug_set_wait_limit", "knng_refine_pointwise_noalloc",
     "knng_build_batch",
@@ -112,6 +112,8 @@ def load_library(path: str = LIB_PATH):
         "knng_process_leaves": (c_int, [P, c_uint32, P, P]),
         "knng_run_rep": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, c_uint32, POINTER(Stats)]),
         "knng_run_rep_kd": (c_int, [P, c_uint32, c_uint32, c_uint64, c_uint32, POINTER(Stats)]),
+        "knng_build_kd": (c_int, [P, P, c_uint32, c_uint32, c_uint64, POINTER(Params), c_uint32, P, P,
+                                  POINTER(Stats)]),
         "knng_kd_rotation": (c_int, [c_uint32, c_uint32, c_uint64, P]),
         "knng_tune_buckets": (c_int, [P, c_uint32, c_uint32, c_uint32, c_uint64, POINTER(ctypes.c_double),
                                       POINTER(c_uint32)]),
@@ -160,6 +162,14 @@ def default_params(**overrides) -> Params:
             raise AttributeError(k)
         setattr(p, k, v)
     return p
+
+
+def kd_params(**overrides) -> Params:
+    """The reference's KD form (src/SolutionRandomKD.hpp:377-430): 5
+    repetitions, buckets below 400 points, no neighbour-of-neighbour pass."""
+    base = dict(reps=5, max_leaf=400, max_leaf_odd=0, refine=0)
+    base.update(overrides)
+    return default_params(**base)
 
 
 def _ptr(a):
@@ -231,6 +241,21 @@ class KnngContext:
         st = stats if stats is not None else Stats()
         self._check(self._lib.knng_build(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p), _ptr(ids),
                                          _ptr(dists), ctypes.byref(st)))
+        self.n, self.d, self.k = n, d, p.k
+        return (ids, dists) if want_dists else ids
+
+    def build_kd(self, points: np.ndarray, params: Params | None = None, new_dims: int = 30,
+                 want_dists: bool = False, stats: Stats | None = None):
+        """knng_build_kd: a whole build with the random-rotation KD splitter
+        (default: the reference's KD form, kd_params())."""
+        pts = _f32(points)
+        n, d = pts.shape
+        p = params or kd_params()
+        ids = np.empty((n, p.k), np.uint32)
+        dists = np.empty((n, p.k), np.float32) if want_dists else None
+        st = stats if stats is not None else Stats()
+        self._check(self._lib.knng_build_kd(self._h, _ptr(pts), n, d, pts.strides[0], ctypes.byref(p), new_dims,
+                                            _ptr(ids), _ptr(dists), ctypes.byref(st)))
         self.n, self.d, self.k = n, d, p.k
         return (ids, dists) if want_dists else ids
 

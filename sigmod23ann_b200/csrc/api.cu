@@ -914,36 +914,85 @@ knng_status knng_kd_rotation(uint32_t new_dims, uint32_t d, uint64_t seed, float
     return KNNG_OK;
 }
 
+namespace knng {
+
+// One KD repetition with its bookkeeping: the context's leaf list and the
+// repetition's statistics.
+void kd_rep_step(Context& c, uint32_t max_leaf, uint32_t new_dims, uint64_t seed, uint32_t rep, knng_stats* stats) {
+    KdRepResult res;
+    run_rep_kd(c, max_leaf, new_dims, seed, rep, res);
+    std::vector<std::pair<uint32_t, uint32_t>> lv(res.leaf_start.size());
+    for (size_t i = 0; i < lv.size(); ++i) lv[i] = {res.leaf_start[i], res.leaf_end[i]};
+    std::sort(lv.begin(), lv.end());
+    c.last_leaf_start.resize(lv.size());
+    c.last_leaf_end.resize(lv.size());
+    for (size_t i = 0; i < lv.size(); ++i) {
+        c.last_leaf_start[i] = lv[i].first;
+        c.last_leaf_end[i] = lv[i].second;
+    }
+    RepStats st;
+    st.levels = res.levels;
+    st.nodes = res.nodes;
+    st.restarts = res.restarts;
+    st.fallbacks = res.fallbacks;
+    st.ms_split = res.ms_split;
+    st.ms_leaf = res.ms_leaf;
+    add_rep_stats(stats, st);
+    if (stats) {
+        stats->reps_done += 1;
+        stats->buckets += lv.size();
+        stats->leaf_launches += lv.empty() ? 0 : 1;
+        stats->ms_leaf_kernel += res.ms_leaf;
+    }
+}
+
+}  // namespace knng
+
 knng_status knng_run_rep_kd(knng_context* ctx, uint32_t max_leaf, uint32_t new_dims, uint64_t seed,
                             uint32_t rep_index, knng_stats* stats) {
     return knng::guarded(ctx, [&](Context& c) {
         if (max_leaf < 2 || max_leaf > 4097) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "max_leaf must be in [2, 4097]");
         knng::require_sets(c);
-        knng::KdRepResult res;
-        knng::run_rep_kd(c, max_leaf, new_dims, seed, rep_index, res);
-        std::vector<std::pair<uint32_t, uint32_t>> lv(res.leaf_start.size());
-        for (size_t i = 0; i < lv.size(); ++i) lv[i] = {res.leaf_start[i], res.leaf_end[i]};
-        std::sort(lv.begin(), lv.end());
-        c.last_leaf_start.resize(lv.size());
-        c.last_leaf_end.resize(lv.size());
-        for (size_t i = 0; i < lv.size(); ++i) {
-            c.last_leaf_start[i] = lv[i].first;
-            c.last_leaf_end[i] = lv[i].second;
+        knng::kd_rep_step(c, max_leaf, new_dims, seed, rep_index, stats);
+    });
+}
+
+knng_status knng_build_kd(knng_context* ctx, const float* points, uint32_t n, uint32_t d, uint64_t ld_bytes,
+                          const knng_params* params, uint32_t new_dims, uint32_t* out_ids, float* out_dists,
+                          knng_stats* stats) {
+    return knng::guarded(ctx, [&](Context& c) {
+        knng::validate_params(params);
+        if (params->precision != KNNG_PRECISION_FP32)
+            knng::fail(KNNG_ERR_INVALID_ARGUMENT, "the KD build computes in FP32");
+        if (new_dims < 1 || new_dims > 32) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "new_dims must be in [1, 32]");
+        if (!out_ids) knng::fail(KNNG_ERR_INVALID_ARGUMENT, "null output");
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        knng::load_points(c, points, n, d, ld_bytes, false, false);
+        knng::alloc_sets(c, params->k);
+        knng::EventPair total_t(c);
+        const uint64_t launches0 = c.launches;
+        for (uint32_t r = 0; r < params->reps; ++r) {
+            const uint32_t leaf = (params->max_leaf_odd != 0 && (r % 2 == 1)) ? params->max_leaf_odd : params->max_leaf;
+            knng::kd_rep_step(c, leaf, new_dims, params->seed, r, stats);
         }
-        knng::RepStats st;
-        st.levels = res.levels;
-        st.nodes = res.nodes;
-        st.restarts = res.restarts;
-        st.fallbacks = res.fallbacks;
-        st.ms_split = res.ms_split;
-        st.ms_leaf = res.ms_leaf;
-        knng::add_rep_stats(stats, st);
+        for (uint32_t pass = 0; pass < params->refine; ++pass) {
+            knng::EventPair rt(c);
+            const uint64_t ch = knng::run_refine(c);
+            knng::add_refine_stats(stats, c, ch, rt.stop(c));
+        }
+        const double ms = total_t.stop(c);
         if (stats) {
-            stats->reps_done += 1;
-            stats->buckets += lv.size();
-            stats->leaf_launches += lv.empty() ? 0 : 1;
-            stats->ms_leaf_kernel += res.ms_leaf;
+            stats->ms_total += ms;
+            stats->kernel_launches += c.launches - launches0;
         }
+        const size_t nk = static_cast<size_t>(c.n) * c.k;
+        knng::EventPair ft(c);
+        uint32_t* d_ids = static_cast<uint32_t*>(knng::scratch(c, "fin_ids", nk * sizeof(uint32_t)));
+        float* d_dist = out_dists ? static_cast<float*>(knng::scratch(c, "fin_dist", nk * sizeof(float))) : nullptr;
+        knng::launch_finalize(c, d_ids, d_dist);
+        if (stats) stats->ms_finalize += ft.stop(c);
+        knng::download(c, out_ids, d_ids, nk);
+        if (out_dists) knng::download(c, out_dists, d_dist, nk);
     });
 }
 

@@ -95,6 +95,7 @@ int main() {
     try {
         knng_b200::constructResult(pts, 4, result);
         knng_b200::constructResultTimed(pts, 4, result, 50, 50);
+        knng_b200::constructResultKD(pts, 4, result);
     } catch (const std::runtime_error& e) {
         std::printf("%s\n", e.what());
         return 3;
@@ -189,3 +190,4 @@ def test_kd_rotation_entry_point_matches_oracle(knng_lib, oracle_lib):
     assert knng_lib.knng_kd_rotation(0, 100, 1, ptr) == 1
     assert knng_lib.knng_kd_rotation(4, 100, 1, None) == 1
     assert knng_lib.knng_run_rep_kd(None, 400, 30, 1, 0, None) == 1
+    assert knng_lib.knng_build_kd(None, None, 0, 100, 0, None, 30, None, None, None) == 1

@@ -640,3 +640,23 @@ def test_kd_rep_matches_oracle(oracle_lib, ctx):
         oids, odist = o.finalize()
         np.testing.assert_array_equal(ids, oids)
         np.testing.assert_array_equal(dist.view(np.uint32), odist.view(np.uint32))
+
+
+def test_build_kd_matches_oracle(oracle_lib, ctx):
+    """knng_build_kd (the reference's KD form as one call: 5 repetitions,
+    buckets below 400, no pass; then a variant with alternating bounds and one
+    pass) gives the oracle's final lists and distances."""
+    from sigmod23ann_b200 import kd_params
+
+    pts = workloads.gaussian_mixture(n=9000, d=100, clusters=20, sigma=0.15, seed=23)
+    for p, leafs in ((kd_params(seed=12345), [400] * 5),
+                     (kd_params(seed=7, reps=3, max_leaf=300, max_leaf_odd=500, refine=1, k=64), [300, 500, 300])):
+        ids, dist = ctx.build_kd(pts, p, want_dists=True)
+        o = oracle_lib.Oracle(pts, k=p.k, rng_mode=1, seed=p.seed)
+        for r, leaf in enumerate(leafs):
+            o.kd_rep(leaf, 30, p.seed, r)
+        for _ in range(p.refine):
+            o.refine()
+        oids, odist = o.finalize()
+        np.testing.assert_array_equal(ids, oids)
+        np.testing.assert_array_equal(dist.view(np.uint32), odist.view(np.uint32))
