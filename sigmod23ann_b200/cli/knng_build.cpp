@@ -2,11 +2,16 @@
 //
 //   knng_build [input.bin] [output.bin] [reps] [refine passes] [max_leaf]
 //   knng_build input.bin output.bin --timed build_ms refine_ms
+//   knng_build input.bin output.bin --kd [reps] [max_leaf]
 //
 // The second form is the reference's wall-clock schedule
 // (SolutionKmeans::constructResult, src/SolutionKmeans.hpp:579-604):
 // repetitions while build_ms has not passed, then passes while
 // build_ms + refine_ms has not (the reference: 1,210,000 and 500,000 ms).
+// The third is the reference's alternative random-rotation KD solution
+// (SolutionRandomKD::constructResult, src/SolutionRandomKD.hpp:377-430):
+// `reps` repetitions (default 5) with buckets below max_leaf (default 400),
+// 30 rotated dimensions, no neighbour-of-neighbour pass.
 //
 // input.bin: uint32 N, then N rows of 100 float32 (the contest format read by
 // ReadBinArray, src/io.h:66-95).  output.bin: N rows of 100 uint32 neighbour
@@ -28,8 +33,14 @@ int main(int argc, char** argv) {
     knng_params p;
     knng_default_params(&p);
     const bool timed = argc > 3 && std::string(argv[3]) == "--timed";
+    const bool kd = argc > 3 && std::string(argv[3]) == "--kd";
     uint64_t build_ms = 0, refine_ms = 0;
-    if (timed) {
+    if (kd) {
+        p.reps = argc > 4 ? static_cast<uint32_t>(std::atoi(argv[4])) : 5u;
+        p.max_leaf = argc > 5 ? static_cast<uint32_t>(std::atoi(argv[5])) : 400u;
+        p.max_leaf_odd = 0;
+        p.refine = 0;
+    } else if (timed) {
         if (argc < 6) {
             std::fprintf(stderr, "usage: knng_build input.bin output.bin --timed build_ms refine_ms\n");
             return 2;
@@ -40,8 +51,8 @@ int main(int argc, char** argv) {
     } else if (argc > 3) {
         p.reps = static_cast<uint32_t>(std::atoi(argv[3]));
     }
-    if (!timed && argc > 4) p.refine = static_cast<uint32_t>(std::atoi(argv[4]));
-    if (!timed && argc > 5) {
+    if (!timed && !kd && argc > 4) p.refine = static_cast<uint32_t>(std::atoi(argv[4]));
+    if (!timed && !kd && argc > 5) {
         p.max_leaf = static_cast<uint32_t>(std::atoi(argv[5]));
         p.max_leaf_odd = 0;
     }
@@ -67,8 +78,9 @@ int main(int argc, char** argv) {
     }
     std::vector<uint32_t> ids(static_cast<size_t>(n) * p.k);
     knng_stats st;
-    s = timed ? knng_build_timed(ctx, pts.data(), n, 100, 400, &p, build_ms, refine_ms, ids.data(), nullptr, &st)
-              : knng_build(ctx, pts.data(), n, 100, 400, &p, ids.data(), nullptr, &st);
+    s = kd      ? knng_build_kd(ctx, pts.data(), n, 100, 400, &p, 30, ids.data(), nullptr, &st)
+        : timed ? knng_build_timed(ctx, pts.data(), n, 100, 400, &p, build_ms, refine_ms, ids.data(), nullptr, &st)
+                : knng_build(ctx, pts.data(), n, 100, 400, &p, ids.data(), nullptr, &st);
     if (s != KNNG_OK) {
         std::fprintf(stderr, "knng_build: %s: %s\n", knng_status_string(s), knng_last_error(ctx));
         knng_destroy(ctx);

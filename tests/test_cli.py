@@ -67,3 +67,18 @@ def test_build_cli_matches_oracle(oracle_lib, knng_lib, tmp_path):
     g = subprocess.run([os.path.join(CLI, "knng_grade"), str(tmp_path / "truth.bin"), str(tmp_path / "out.bin"),
                         "2500"], capture_output=True, text=True, check=True)
     assert "recall: 1.000000" in g.stdout
+
+
+@pytest.mark.gpu
+def test_build_cli_kd_form_matches_oracle(oracle_lib, knng_lib, tmp_path):
+    """--kd: the reference's KD solution (5 repetitions of the random-rotation
+    KD split by default; here 3, buckets below 300), no top-up."""
+    pts = workloads.gaussian_mixture(n=2500, d=100, clusters=8, sigma=0.15, seed=32)
+    write_contest_file(tmp_path / "in.bin", pts)
+    subprocess.run([os.path.join(CLI, "knng_build"), str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), "--kd", "3",
+                    "300"], check=True, capture_output=True)
+    ids = np.fromfile(tmp_path / "out.bin", dtype=np.uint32).reshape(2500, 100)
+    o = oracle_lib.Oracle(pts, k=100, rng_mode=1, seed=12345)
+    for r in range(3):
+        o.kd_rep(300, 30, 12345, r)
+    np.testing.assert_array_equal(ids, o.finalize()[0])
