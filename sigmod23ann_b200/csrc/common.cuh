@@ -301,16 +301,17 @@ __device__ __forceinline__ uint32_t set_offer_batch(WarpSet& s, uint32_t cand, f
     return changed;
 }
 
-// Ascending bitonic sort of n (power of two, n >= 2) 64-bit keys by one warp;
-// keys may live in shared or global memory.
-__device__ __forceinline__ void warp_bitonic_sort(unsigned long long* keys, uint32_t n, int lane) {
+// Ascending bitonic sort of n (power of two, n >= 2) unsigned keys by one
+// warp; keys may live in shared or global memory.
+template <class Key>
+__device__ __forceinline__ void warp_bitonic_sort(Key* keys, uint32_t n, int lane) {
     for (uint32_t k = 2; k <= n; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             for (uint32_t t = lane; t < n / 2; t += kWarp) {
                 const uint32_t i = 2 * t - (t & (j - 1));  // 2 j (t / j) + t % j, j a power of two
                 const uint32_t partner = i + j;
                 const bool up = (i & k) == 0;
-                const unsigned long long a = keys[i], b = keys[partner];
+                const Key a = keys[i], b = keys[partner];
                 if ((a > b) == up) {
                     keys[i] = b;
                     keys[partner] = a;

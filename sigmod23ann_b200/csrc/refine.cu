@@ -81,16 +81,16 @@ __global__ void __launch_bounds__(kSnapWarps * kWarp) k_snapshot(const uint32_t*
                                                                  uint32_t* __restrict__ snap,
                                                                  const uint32_t* __restrict__ prev,
                                                                  uint32_t* __restrict__ old) {
-    __shared__ unsigned long long keys_s[kSnapWarps][kMaxK];
+    __shared__ uint32_t keys_s[kSnapWarps][kMaxK];
     __shared__ uint32_t prev_s[kSnapWarps][kMaxK];
     const int lane = threadIdx.x % kWarp, warp = threadIdx.x / kWarp;
-    unsigned long long* keys = keys_s[warp];
+    uint32_t* keys = keys_s[warp];
     uint32_t* pl = prev_s[warp];
     int top = 1;  // largest power of two <= K (branch-free lower bound)
     while (top * 2 <= K) top *= 2;
     for (uint32_t p = blockIdx.x * kSnapWarps + warp; p < n; p += gridDim.x * kSnapWarps) {
         const size_t base = static_cast<size_t>(p) * K;
-        for (int slot = lane; slot < kMaxK; slot += kWarp) keys[slot] = slot < K ? set_id[base + slot] : ~0ull;
+        for (int slot = lane; slot < kMaxK; slot += kWarp) keys[slot] = slot < K ? set_id[base + slot] : ~0u;
         if (prev)
             for (int i = lane; i < K; i += kWarp) pl[i] = prev[base + i];
         __syncwarp();
