@@ -294,12 +294,9 @@ __device__ __forceinline__ uint32_t set_offer_batch(WarpSet& s, uint32_t cand, f
         pending &= pending - 1;
         const float dj = __shfl_sync(kFull, d, src);
         const uint32_t cj = __shfl_sync(kFull, cand, src);
-        // The bound changes only when an offer is taken; it only decreases:
-        // then drop the candidates it now excludes.
-        if (dj < s.bound && set_offer(s, cj, dj, K, lane)) {
-            ++changed;
-            pending &= __ballot_sync(kFull, valid && d < s.bound);
-        }
+        if (dj < s.bound) changed += set_offer(s, cj, dj, K, lane) ? 1u : 0u;
+        // The bound only decreases: drop the candidates it now excludes.
+        pending &= __ballot_sync(kFull, valid && d < s.bound);
     }
     return changed;
 }
