@@ -242,3 +242,26 @@ def test_lloyd_sums_follow_point_order(oracle_lib):
     assert ok
     # c1 = (0.5, 1000, 0, ...), c2 = (0, -1000, 0.5, ...): coefs = (c1 - c2) / 2.
     assert coefs[0] == np.float32(0.25) and coefs[2] == np.float32(-0.25) and coefs[1] == np.float32(1000.0)
+
+
+def test_kd_oracle_edge_cases(oracle_lib):
+    """One bucket when n < max_leaf (every pair offered); one rotated
+    dimension; the same seed and repetition give the same permutation, another
+    repetition (another rotation and draws) a different one."""
+    pts = workloads.gaussian_mixture(n=150, d=100, clusters=3, sigma=0.3, seed=9)
+    o = oracle_lib.Oracle(pts, k=10, rng_mode=1, seed=1)
+    o.kd_rep(400, 30, 1, 0)
+    t = o.trace()
+    assert t["leaf_start"].tolist() == [0] and t["leaf_end"].tolist() == [150]
+    assert np.array_equal(o.indices(), np.arange(150))
+    assert (o.sets()["size"] == 10).all()
+    big = workloads.gaussian_mixture(n=2000, d=100, clusters=6, sigma=0.2, seed=10)
+    a = oracle_lib.Oracle(big, k=10, rng_mode=1, seed=1)
+    a.kd_rep(200, 1, 5, 0)
+    ta = a.trace()
+    assert (ta["leaf_end"] - ta["leaf_start"]).max() < 200
+    b = oracle_lib.Oracle(big, k=10, rng_mode=1, seed=1)
+    b.kd_rep(200, 1, 5, 0)
+    assert np.array_equal(a.indices(), b.indices())
+    b.kd_rep(200, 1, 5, 1)
+    assert not np.array_equal(a.indices(), b.indices())
