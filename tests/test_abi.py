@@ -38,6 +38,14 @@ def test_default_params_are_the_references(knng_lib):
     assert p.refine == 1 and p.precision == api.PRECISION_FP32
 
 
+def test_kd_params_are_the_kd_forms(knng_lib):
+    """kd_params(): the reference's KD form (src/SolutionRandomKD.hpp:390-401):
+    five repetitions, buckets below 400 points, no neighbour-of-neighbour pass."""
+    p = api.kd_params()
+    assert (p.k, p.reps, p.max_leaf, p.max_leaf_odd, p.refine, p.seed) == (100, 5, 400, 0, 0, 12345)
+    assert api.kd_params(reps=2, k=10).reps == 2
+
+
 def test_status_strings(knng_lib):
     for code in range(9):
         assert knng_lib.knng_status_string(code)
